@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Benchmark of the RF -> volume pipeline (one JSON line on rank 0).
+
+Workload ("full"): 128 transmits x 128 receive channels x 4096 samples of Hadamard-encoded
+int16 RF (128 MiB raw), 64-tap chirp match filter, HERCULES plane-wave delay-and-sum into a
+128 x 128 x 256 complex64 volume with cubic interpolation and coherence-factor weighting.
+One step = convert + reorder + decode -> Hilbert -> delay-and-sum of one frame.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (launched by torchrun) every rank beamforms its own frames (frames are
+independent: no collective on the data path) and the job-wide volumes/s is reported
+(weak scaling). --impl reference times the CPU path (the FP64 oracle) on a bounded
+sample of the same workload on rank 0.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "volumes/s (plain full-transmit RF->volume pipeline)"
+UNIT = "volumes/s"
+WORKLOAD = "full"
+
+
+def workload_config(extra=None):
+    from cuda_ultrasound_toolkit_b200 import synth
+    w = synth.CONFIGS[WORKLOAD]
+    cfg = {"workload": "rca128_hercules_cubic_cf", "transmits": w.T, "channels": w.C, "samples": w.S,
+           "volume": [w.X, w.Y, w.Z], "input": "int16 Hadamard-encoded", "match_filter_taps": w.filter_taps,
+           "interpolation": "cubic", "coherence_factor": w.cf,
+           "l2": "inputs > L2 (128 MiB raw, 512 MiB analytic signal; two raw frames alternate)"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ---- clocks sampled during the timed region ------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "of measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "of fallback"
+
+
+def profile_traffic(name):
+    """DRAM bytes per launch recorded by ncu for a kernel (profiles/<name>.json), if committed."""
+    path = os.path.join(ROOT, "profiles", f"{name}.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    return None
+
+
+# ---- CPU reference arm -------------------------------------------------------------------------------
+def cpu_sample(raw, bp, threads, frac_rows=1 / 8, frac_vox=1 / 128, seed=0):
+    """Times the FP64 oracle on a bounded sample and extrapolates seconds per volume."""
+    from oracle import oracle as O
+    S, C, T = bp.dims
+    z, y, x = bp.volume_shape
+    sub_c = max(1, int(round(C * frac_rows)))
+    sub = bp.copy()
+    sub.dec_data_dim[1] = sub_c
+    t0 = time.perf_counter()
+    dec = O.decode_f64(raw, sub, threads)
+    t1 = time.perf_counter()
+    taps = np.ctypeslib.as_array(bp.rf_filter)[: int(bp.filter_length)].astype(np.float32)
+    iq_sub = O.hilbert(dec, taps if len(taps) else None, threads)
+    t2 = time.perf_counter()
+    # delay-and-sum needs every row: tile the sampled channels to the full aperture
+    iq = np.empty((T, C, S), np.complex128)
+    for c in range(C):
+        iq[:, c] = iq_sub[:, c % sub_c]
+    rng = np.random.default_rng(seed)
+    n_vox = max(1, int(x * y * z * frac_vox))
+    vox = rng.choice(x * y * z, n_vox, replace=False)
+    t3 = time.perf_counter()
+    O.das(iq, bp, vox, threads)
+    t4 = time.perf_counter()
+    per_volume = (t1 - t0) / (sub_c / C) + (t2 - t1) / (sub_c / C) + (t4 - t3) / (n_vox / (x * y * z))
+    sample = (f"decode+Hilbert of {sub_c}/{C} receive channels, delay-and-sum of {n_vox} random voxels "
+              f"of {x * y * z}; extrapolated linearly to one volume")
+    return per_volume, sample
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    from cuda_ultrasound_toolkit_b200 import synth
+    raw, bp = synth.frame(WORKLOAD)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_sample(raw, bp, threads, frac_rows=1 / 64, frac_vox=1 / 4096)
+    times = []
+    sample = ""
+    for k in range(args.steps):
+        sec, sample = cpu_sample(raw, bp, threads, frac_rows=1 / 32, frac_vox=1 / 2048, seed=k)
+        times.append(sec)
+    value = len(times) / sum(times)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded phantom, 200 point scatterers, 40 dB SNR)",
+            "config": workload_config({"parallelism": "cpu threads"}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---- GPU arm ------------------------------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from cuda_ultrasound_toolkit_b200 import Plan, beamform, synth
+    from cuda_ultrasound_toolkit_b200.api import calibrate_fp32
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    frames = [synth.frame(WORKLOAD, seed=7000 + 2 * rank + k) for k in range(2)]
+    bp = frames[0][1]
+    for _, b in frames[1:]:  # same geometry; only the data and channel map differ per frame
+        assert b.dims == bp.dims
+    plans = [Plan(b) for _, b in frames]
+    d_raw = [torch.from_numpy(r).to(dev) for r, _ in frames]
+    vol = plans[0].empty_volume()
+    stream = torch.cuda.current_stream()
+
+    def step(k):
+        plans[k % 2].beamform(d_raw[k % 2], out=vol, stream=stream)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(args.steps):
+        step(k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clock = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    launches = plans[0].launches * args.steps
+
+    # Per-stage timing on the same stream (dominant kernel = delay-and-sum).
+    p = plans[0]
+    dec = p.empty_decoded()
+    iq = p.empty_iq()
+    stage_ms = {}
+    for name, fn in (("decode", lambda: p.decode(d_raw[0], out=dec, stream=stream)),
+                     ("hilbert", lambda: p.hilbert(dec, out=iq, stream=stream)),
+                     ("das", lambda: p.das(iq, out=vol, stream=stream))):
+        fn()
+        reps = 3 if name == "das" else 20
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        stage_ms[name] = a.elapsed_time(b) / reps
+
+    # End to end through the host-span entry point (cuda_toolkit::beamform): pinned host
+    # input, H2D copy, pipeline, D2H of the volume, every step.
+    host_raw = [torch.from_numpy(r).pin_memory() for r, _ in frames]
+    host_vol = torch.empty(bp.volume_shape, dtype=torch.complex64).pin_memory()
+    raw_np = [h.numpy() for h in host_raw]
+    vol_np = host_vol.numpy()
+    for k in range(2):
+        beamform(raw_np[k % 2], frames[k % 2][1], out=vol_np)
+    e2e_steps = max(3, args.steps // 2)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        beamform(raw_np[k % 2], frames[k % 2][1], out=vol_np)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    barrier()
+
+    # Max over ranks.
+    if world > 1:
+        t = torch.tensor([ms, e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_s = t.tolist()
+    if rank != 0:
+        return
+
+    S, C, T = bp.dims
+    z, y, x = bp.volume_shape
+    vct = x * y * z * T * C
+    flops_per_vct = 49 if bp.interpolate else 23  # cubic + CF / linear, no CF
+    if bp.interpolate and bp.coherency_weighting <= 0:
+        flops_per_vct = 45
+    fp32_peak = calibrate_fp32()
+    das_tflops = vct * flops_per_vct / (stage_ms["das"] * 1e-3) / 1e12
+    peaks, peak_src = measured_peaks()
+    hbm = peaks["hbm_gbs"]
+    dec_bytes = T * C * S * (2 + 4)
+    hil_bytes = T * C * S * (4 + 8)
+    value = args.steps * world / (ms * 1e-3)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (int16 input, int32 exact decode)",
+        "data": "synthetic (seeded phantom, 200 point scatterers, 40 dB SNR)",
+        "config": workload_config({"parallelism": f"frame-parallel x{world}" if world > 1 else "single GPU"}),
+        "e2e": {"value": e2e_steps * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(raw_np[0].nbytes),
+                "d2h_bytes_per_step": int(vol_np.nbytes), "api": "cuda_toolkit::beamform (host spans)"},
+        "roofline": {"bound": "fp32", "kernel": "das", "achieved": das_tflops, "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": das_tflops / fp32_peak, "traffic": profile_traffic("das_full"),
+                     "algorithmic": f"{flops_per_vct} FLOP per voxel-transmit-channel x {vct} per launch",
+                     "peak_source": "measured FP32 FMA probe (cutb_calibrate_fp32) on this GPU"},
+        "stages": {
+            "decode": {"ms": stage_ms["decode"], "achieved_gbs": dec_bytes / (stage_ms["decode"] * 1e-3) / 1e9,
+                       "peak_gbs": hbm, "frac": dec_bytes / (stage_ms["decode"] * 1e-3) / 1e9 / hbm,
+                       "peak_note": peak_src, "traffic": profile_traffic("decode_full")},
+            "hilbert": {"ms": stage_ms["hilbert"], "achieved_gbs": hil_bytes / (stage_ms["hilbert"] * 1e-3) / 1e9,
+                        "peak_gbs": hbm, "frac": hil_bytes / (stage_ms["hilbert"] * 1e-3) / 1e9 / hbm,
+                        "peak_note": peak_src, "traffic": profile_traffic("hilbert_full")},
+            "das": {"ms": stage_ms["das"], "tflops": das_tflops},
+        },
+        "gpu_launches": launches,
+        "clocks": clock,
+    }
+    try:
+        per_vol, sample = cpu_sample(frames[0][0], bp, os.cpu_count() or 1)
+        line["cpu_baseline"] = {"value": 1.0 / per_vol, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+                                "sample": sample}
+    except Exception as exc:  # the baseline must not hide the GPU number
+        line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                "sample": f"failed: {exc}"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,278 @@
+"""Python host mirror of the library's C ABI.
+
+Three layers, all calling libcuda_toolkit_b200.so through ctypes (no CPU fallback: a
+missing or unloadable library raises):
+
+* ``beamform`` / ``beamform_i16`` / ``beamform_f32``: host arrays in, host volume out,
+  through the upstream-compatible entry points (cuda_toolkit::beamform and the MATLAB
+  wrappers; upstream cuda_toolkit/src/api/cuda_toolkit.cpp:109-199,
+  cuda_toolkit_matlab.cpp:9-37).
+* ``Plan``: the device-resident stages (cutb_decode / cutb_hilbert / cutb_das /
+  cutb_beamform) on torch CUDA tensors and the current torch stream.
+* ``RfSession``: the buffer-registry front end (init_cuda_configuration ... cuda_hilbert;
+  upstream cuda_toolkit_ogl.cpp:105-273), with device tensors standing in for GL buffers.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .params import CudaBeamformerParameters, InputDataTypes, MAX_CHANNEL_COUNT
+
+_LIB_NAME = "libcuda_toolkit_b200.so"
+_lib = None
+
+
+class CutbError(RuntimeError):
+    """A library call returned false; ``code`` is cutb_last_error()."""
+
+    def __init__(self, what, code, message):
+        super().__init__(f"{what} failed (code {code}): {message}")
+        self.code = code
+        self.message = message
+
+
+def library_path():
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), _LIB_NAME)
+
+
+def lib():
+    """Loads the native library once; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `make -C {os.path.dirname(path)}`")
+    L = ctypes.CDLL(path)
+    P = ctypes.POINTER(CudaBeamformerParameters)
+    vp, sz, u, b = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint, ctypes.c_bool
+    sig = {
+        "cutb_last_error": ([], ctypes.c_int),
+        "cutb_last_error_message": ([], ctypes.c_char_p),
+        "cutb_clear_error": ([], None),
+        "cutb_version": ([], ctypes.c_int),
+        "cutb_encoding_matrix": ([u, ctypes.c_int, ctypes.POINTER(ctypes.c_int8)], b),
+        "cutb_plan_create": ([P, vp], vp),
+        "cutb_plan_destroy": ([vp], None),
+        "cutb_plan_raw_bytes": ([vp], sz),
+        "cutb_plan_iq_bytes": ([vp], sz),
+        "cutb_plan_volume_bytes": ([vp], sz),
+        "cutb_plan_last_launch_count": ([vp], ctypes.c_int),
+        "cutb_decode": ([vp, vp, sz, vp, u, vp], b),
+        "cutb_hilbert": ([vp, vp, u, vp, vp], b),
+        "cutb_das": ([vp, vp, vp, vp], b),
+        "cutb_beamform": ([vp, vp, sz, vp, vp], b),
+        "cutb_debug_fail_allocations_after": ([ctypes.c_int], None),
+        "cutb_calibrate_fp32": ([ctypes.POINTER(ctypes.c_double), vp], b),
+        "init_cuda_configuration": ([ctypes.POINTER(u), ctypes.POINTER(u)], b),
+        "register_cuda_buffers": ([ctypes.POINTER(u), u, u], b),
+        "cuda_set_channel_mapping": ([ctypes.POINTER(ctypes.c_int16)], b),
+        "cuda_set_match_filter": ([ctypes.POINTER(ctypes.c_float), u], b),
+        "cuda_hilbert": ([u, u], b),
+        "cuda_decode": ([sz, u], b),
+        "deinit_cuda_configuration": ([], None),
+        "cuda_register_device_buffer": ([u, vp, sz], b),
+        "beamform_i16_matlab": ([vp, CudaBeamformerParameters, vp], None),
+        "beamform_f32_matlab": ([vp, CudaBeamformerParameters, vp], None),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    # cuda_toolkit::beamform(std::span<const u8>, std::span<u8>, const CudaBeamformerParameters&):
+    # on x86-64 SysV each span (pointer, size) travels in two integer registers.
+    cxx = getattr(L, "_ZN12cuda_toolkit8beamformESt4spanIKhLm18446744073709551615EES0_IhLm18446744073709551615EERK24CudaBeamformerParameters")
+    cxx.argtypes = [vp, sz, vp, sz, P]
+    cxx.restype = b
+    L.cxx_beamform = cxx
+    _lib = L
+    return L
+
+
+def last_error():
+    L = lib()
+    return L.cutb_last_error(), L.cutb_last_error_message().decode(errors="replace")
+
+
+def _check(ok, what):
+    if not ok:
+        code, msg = last_error()
+        raise CutbError(what, code, msg)
+
+
+def encoding_matrix(n, ordering=1):
+    """Order-n transmit encoding matrix (+1/-1 int8, rows in output order)."""
+    out = np.empty((n, n), dtype=np.int8)
+    _check(lib().cutb_encoding_matrix(n, ordering, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int8))),
+           "cutb_encoding_matrix")
+    return out
+
+
+def calibrate_fp32(stream=None):
+    """Measured FP32 FMA throughput of the current device, TFLOP/s."""
+    v = ctypes.c_double()
+    _check(lib().cutb_calibrate_fp32(ctypes.byref(v), _stream_handle(stream)), "cutb_calibrate_fp32")
+    return v.value
+
+
+# ---- host-span entry points --------------------------------------------------------------------
+def beamform(raw, bp: CudaBeamformerParameters, out=None):
+    """cuda_toolkit::beamform on host arrays; returns the complex64 volume [Z][Y][X]."""
+    raw = np.ascontiguousarray(raw)
+    if out is None:
+        out = np.empty(bp.volume_shape, dtype=np.complex64)
+    _check(lib().cxx_beamform(raw.ctypes.data, raw.nbytes, out.ctypes.data, out.nbytes, ctypes.byref(bp)),
+           "cuda_toolkit::beamform")
+    return out
+
+
+def beamform_i16(raw, bp, out=None):
+    """beamform_i16_matlab (errors are only logged upstream; here they raise)."""
+    raw = np.ascontiguousarray(raw, dtype=np.int16)
+    if out is None:
+        out = np.empty(bp.volume_shape, dtype=np.complex64)
+    lib().cutb_clear_error()
+    lib().beamform_i16_matlab(raw.ctypes.data, bp, out.ctypes.data)
+    code, msg = last_error()
+    if code:
+        raise CutbError("beamform_i16_matlab", code, msg)
+    return out
+
+
+def beamform_f32(raw, bp, out=None):
+    raw = np.ascontiguousarray(raw, dtype=np.float32)
+    if out is None:
+        out = np.empty(bp.volume_shape, dtype=np.complex64)
+    lib().cutb_clear_error()
+    lib().beamform_f32_matlab(raw.ctypes.data, bp, out.ctypes.data)
+    code, msg = last_error()
+    if code:
+        raise CutbError("beamform_f32_matlab", code, msg)
+    return out
+
+
+# ---- device-resident stages ----------------------------------------------------------------------
+class _Options(ctypes.Structure):
+    _fields_ = [("iq_bf16", ctypes.c_int), ("das_tile", ctypes.c_int), ("reserved", ctypes.c_int * 14)]
+
+
+def _stream_handle(stream):
+    import torch
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+class Plan:
+    """cutb_plan over torch CUDA tensors. Stage calls are asynchronous on `stream`
+    (default: the current torch stream)."""
+
+    def __init__(self, bp: CudaBeamformerParameters, iq_bf16=False, das_tile=0):
+        import torch  # noqa: F401  (device memory comes from torch)
+        self.bp = bp.copy()
+        opts = _Options(int(iq_bf16), int(das_tile))
+        self._h = lib().cutb_plan_create(ctypes.byref(self.bp), ctypes.byref(opts))
+        _check(self._h, "cutb_plan_create")
+        self.iq_bf16 = bool(iq_bf16)
+        self.raw_bytes = lib().cutb_plan_raw_bytes(self._h)
+        self.iq_bytes = lib().cutb_plan_iq_bytes(self._h)
+        self.volume_bytes = lib().cutb_plan_volume_bytes(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cutb_plan_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    @property
+    def launches(self):
+        return lib().cutb_plan_last_launch_count(self._h)
+
+    # Allocation helpers -------------------------------------------------------------------------
+    def empty_decoded(self, out_stride=1):
+        import torch
+        S, C, T = self.bp.dims
+        return torch.empty((T, C, S * out_stride), dtype=torch.float32, device="cuda")
+
+    def empty_iq(self):
+        import torch
+        S, C, T = self.bp.dims
+        if self.iq_bf16:
+            return torch.empty((T, C, S, 2), dtype=torch.bfloat16, device="cuda")
+        return torch.empty((T, C, S), dtype=torch.complex64, device="cuda")
+
+    def empty_volume(self):
+        import torch
+        return torch.empty(self.bp.volume_shape, dtype=torch.complex64, device="cuda")
+
+    # Stages ------------------------------------------------------------------------------------
+    def decode(self, raw, out=None, out_stride=1, stream=None):
+        out = self.empty_decoded(out_stride) if out is None else out
+        _check(lib().cutb_decode(self._h, raw.data_ptr(), raw.numel() * raw.element_size(), out.data_ptr(),
+                                 out_stride, _stream_handle(stream)), "cutb_decode")
+        return out
+
+    def hilbert(self, decoded, in_stride=1, out=None, stream=None):
+        out = self.empty_iq() if out is None else out
+        _check(lib().cutb_hilbert(self._h, decoded.data_ptr(), in_stride, out.data_ptr(), _stream_handle(stream)),
+               "cutb_hilbert")
+        return out
+
+    def das(self, iq, out=None, stream=None):
+        out = self.empty_volume() if out is None else out
+        _check(lib().cutb_das(self._h, iq.data_ptr(), out.data_ptr(), _stream_handle(stream)), "cutb_das")
+        return out
+
+    def beamform(self, raw, out=None, stream=None):
+        out = self.empty_volume() if out is None else out
+        _check(lib().cutb_beamform(self._h, raw.data_ptr(), raw.numel() * raw.element_size(), out.data_ptr(),
+                                   _stream_handle(stream)), "cutb_beamform")
+        return out
+
+
+# ---- buffer-registry front end ------------------------------------------------------------------
+class RfSession:
+    """init_cuda_configuration / register_cuda_buffers / cuda_decode / cuda_hilbert with torch
+    tensors registered as the 'GL buffers' (ids are assigned here)."""
+
+    def __init__(self, raw_dims, dec_dims):
+        L = lib()
+        self._ids = {}
+        self._next = 1
+        _check(L.init_cuda_configuration((ctypes.c_uint * 2)(*raw_dims), (ctypes.c_uint * 3)(*dec_dims)),
+               "init_cuda_configuration")
+
+    def register(self, tensor):
+        bid = self._next
+        self._next += 1
+        _check(lib().cuda_register_device_buffer(bid, tensor.data_ptr(), tensor.numel() * tensor.element_size()),
+               "cuda_register_device_buffer")
+        self._ids[bid] = tensor
+        return bid
+
+    def register_buffers(self, rf_ids, raw_id):
+        _check(lib().register_cuda_buffers((ctypes.c_uint * max(1, len(rf_ids)))(*rf_ids), len(rf_ids), raw_id),
+               "register_cuda_buffers")
+
+    def set_channel_mapping(self, mapping):
+        m = np.zeros(MAX_CHANNEL_COUNT, dtype=np.int16)
+        m[: len(mapping)] = mapping
+        _check(lib().cuda_set_channel_mapping(m.ctypes.data_as(ctypes.POINTER(ctypes.c_int16))),
+               "cuda_set_channel_mapping")
+
+    def set_match_filter(self, taps):
+        taps = np.ascontiguousarray(taps, dtype=np.float32)
+        _check(lib().cuda_set_match_filter(taps.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), len(taps)),
+               "cuda_set_match_filter")
+
+    def decode(self, input_offset, out_idx):
+        _check(lib().cuda_decode(input_offset, out_idx), "cuda_decode")
+
+    def hilbert(self, in_idx, out_idx):
+        _check(lib().cuda_hilbert(in_idx, out_idx), "cuda_hilbert")
+
+    def close(self):
+        lib().deinit_cuda_configuration()
+        self._ids.clear()

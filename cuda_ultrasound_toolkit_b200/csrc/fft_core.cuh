@@ -1,0 +1,201 @@
+// Shared-memory Stockham FFT building blocks for one power-of-two row of N points,
+// held by N/16 threads with 16 complex values each.
+//
+// Invariant between passes: thread tau holds element n = tau + m*(N/16) in register
+// x[m] (m = 0..15) before the first pass and after the last one, for every radix
+// sequence. That lets a forward and an inverse transform run back to back with the
+// spectrum staying in registers (spectral multiply in between), and makes the first
+// global load and the last global store coalesced across threads.
+//
+// Pass with radix R after `ns` points have been combined: butterfly j in [0, N/R)
+// reads elements j + r*N/R (r < R), twiddles them by w^(r*(j mod ns)) with
+// w = exp(sign*2*pi*i/(ns*R)), runs an R-point DFT and writes element
+// (j/ns)*ns*R + (j mod ns) + r*ns. Thread tau runs butterflies j = tau + u*N/16,
+// u < 16/R, whose inputs are exactly its registers x[u + r*16/R].
+//
+// All functions are __host__ __device__ so a CPU test can drive the same arithmetic.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace cutb {
+namespace fft {
+
+struct cplx {
+    float x, y;
+};
+
+__host__ __device__ __forceinline__ cplx cadd(cplx a, cplx b) { return {a.x + b.x, a.y + b.y}; }
+__host__ __device__ __forceinline__ cplx csub(cplx a, cplx b) { return {a.x - b.x, a.y - b.y}; }
+__host__ __device__ __forceinline__ cplx cmul(cplx a, cplx b)
+{
+    return {fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x)};
+}
+// Multiply by (sign * i): sign = -1 -> -i, +1 -> +i.
+template <int SIGN>
+__host__ __device__ __forceinline__ cplx mul_i(cplx a)
+{
+    if constexpr (SIGN < 0) return {a.y, -a.x};
+    else return {-a.y, a.x};
+}
+
+// exp(SIGN * 2*pi*i * k / 16) for the fixed angles used inside the 8- and 16-point DFTs.
+template <int SIGN>
+__host__ __device__ __forceinline__ cplx w16(int k)
+{
+    constexpr float c1 = 0.92387953251128674f, s1 = 0.38268343236508978f, h = 0.70710678118654752f;
+    float re, im;
+    switch (k & 15) {
+        case 0: re = 1.f; im = 0.f; break;
+        case 1: re = c1; im = s1; break;
+        case 2: re = h; im = h; break;
+        case 3: re = s1; im = c1; break;
+        case 4: re = 0.f; im = 1.f; break;
+        case 5: re = -s1; im = c1; break;
+        case 6: re = -h; im = h; break;
+        case 7: re = -c1; im = s1; break;
+        case 8: re = -1.f; im = 0.f; break;
+        case 9: re = -c1; im = -s1; break;
+        case 10: re = -h; im = -h; break;
+        case 11: re = -s1; im = -c1; break;
+        case 12: re = 0.f; im = -1.f; break;
+        case 13: re = s1; im = -c1; break;
+        case 14: re = h; im = -h; break;
+        default: re = c1; im = -s1; break;
+    }
+    return {re, SIGN < 0 ? -im : im};
+}
+
+template <int SIGN>
+__host__ __device__ __forceinline__ void dft2(cplx& a, cplx& b)
+{
+    cplx t = a;
+    a = cadd(t, b);
+    b = csub(t, b);
+}
+
+template <int SIGN>
+__host__ __device__ __forceinline__ void dft4(cplx& a, cplx& b, cplx& c, cplx& d)
+{
+    cplx t0 = cadd(a, c), t1 = csub(a, c), t2 = cadd(b, d), t3 = mul_i<SIGN>(csub(b, d));
+    a = cadd(t0, t2);
+    c = csub(t0, t2);
+    b = cadd(t1, t3);
+    d = csub(t1, t3);
+}
+
+// In-place R-point DFT of v[0..R-1], natural input and output order.
+template <int R, int SIGN>
+__host__ __device__ __forceinline__ void dft(cplx (&v)[R])
+{
+    if constexpr (R == 2) {
+        dft2<SIGN>(v[0], v[1]);
+    } else if constexpr (R == 4) {
+        dft4<SIGN>(v[0], v[1], v[2], v[3]);
+    } else if constexpr (R == 8) {
+        // Even/odd split: two 4-point DFTs, then the radix-2 combination with w8^k.
+        cplx e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+        dft4<SIGN>(e[0], e[1], e[2], e[3]);
+        dft4<SIGN>(o[0], o[1], o[2], o[3]);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            cplx t = k == 0 ? o[0] : cmul(o[k], w16<SIGN>(2 * k));
+            v[k] = cadd(e[k], t);
+            v[k + 4] = csub(e[k], t);
+        }
+    } else {
+        static_assert(R == 16, "radix");
+        // 16 = 4 x 4: DFT over n1 of v[4*n1 + n2], twiddle w16^(n2*k1), DFT over n2.
+        cplx y[4][4];
+#pragma unroll
+        for (int n2 = 0; n2 < 4; ++n2) {
+            cplx a = v[n2], b = v[4 + n2], c = v[8 + n2], d = v[12 + n2];
+            dft4<SIGN>(a, b, c, d);
+            y[0][n2] = a; y[1][n2] = b; y[2][n2] = c; y[3][n2] = d;
+        }
+#pragma unroll
+        for (int k1 = 1; k1 < 4; ++k1)
+#pragma unroll
+            for (int n2 = 1; n2 < 4; ++n2) y[k1][n2] = cmul(y[k1][n2], w16<SIGN>(n2 * k1));
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) {
+            dft4<SIGN>(y[k1][0], y[k1][1], y[k1][2], y[k1][3]);
+            v[k1] = y[k1][0];
+            v[k1 + 4] = y[k1][1];
+            v[k1 + 8] = y[k1][2];
+            v[k1 + 12] = y[k1][3];
+        }
+    }
+}
+
+// Radix of pass p for a transform of size N = 2^logn: radix-16 passes first, the
+// remaining factor (2, 4 or 8) last.
+__host__ __device__ constexpr int pass_count(int logn) { return logn / 4 + (logn % 4 ? 1 : 0); }
+__host__ __device__ constexpr int pass_radix(int logn, int p) { return p < logn / 4 ? 16 : 1 << (logn % 4); }
+__host__ __device__ constexpr int pass_ns_log(int logn, int p) { return 4 * p; }  // log2 of points combined before pass p
+
+// Padded shared-memory index: one float of padding every 32 floats.
+__host__ __device__ __forceinline__ uint32_t spad(uint32_t i) { return i + (i >> 5); }
+__host__ __device__ constexpr uint32_t spad_size(uint32_t n) { return n + (n >> 5) + 1; }
+
+// Butterflies of pass p for thread tau, reading and writing registers x[]. For the last
+// pass the results stay in registers (natural order); otherwise they are scattered to
+// the shared arrays sre/sim at their output positions. tw = exp(-2*pi*i*m/N), m < N.
+template <int LOGN, int P, int SIGN>
+__host__ __device__ __forceinline__ void fft_pass(cplx (&x)[16], uint32_t tau, const cplx* __restrict__ tw,
+                                                  float* sre, float* sim)
+{
+    constexpr int N = 1 << LOGN;
+    constexpr int TPF = N / 16;
+    constexpr int R = pass_radix(LOGN, P);
+    constexpr int B = 16 / R;
+    constexpr int NS_LOG = pass_ns_log(LOGN, P);
+    constexpr int NS = 1 << NS_LOG;
+    constexpr bool LAST = P == pass_count(LOGN) - 1;
+    constexpr int TW_SHIFT = LOGN - NS_LOG - (R == 16 ? 4 : R == 8 ? 3 : R == 4 ? 2 : 1);  // log2(N/(ns*R))
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+        const uint32_t j = tau + u * TPF;
+        const uint32_t k = j & (NS - 1);
+        cplx v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = x[u + r * B];
+        if constexpr (P > 0) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                cplx w = tw[(r * k) << TW_SHIFT];
+                if constexpr (SIGN > 0) w.y = -w.y;
+                v[r] = cmul(v[r], w);
+            }
+        }
+        dft<R, SIGN>(v);
+        if constexpr (LAST) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) x[u + r * B] = v[r];
+        } else {
+            const uint32_t base = (j >> NS_LOG) * (NS * R) + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const uint32_t pos = spad(base + r * NS);
+                sre[pos] = v[r].x;
+                sim[pos] = v[r].y;
+            }
+        }
+    }
+}
+
+// Gather this thread's 16 elements (tau + m*N/16) back from shared memory.
+template <int LOGN>
+__host__ __device__ __forceinline__ void fft_gather(cplx (&x)[16], uint32_t tau, const float* sre, const float* sim)
+{
+    constexpr int TPF = (1 << LOGN) / 16;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const uint32_t pos = spad(tau + m * TPF);
+        x[m] = {sre[pos], sim[pos]};
+    }
+}
+
+}  // namespace fft
+}  // namespace cutb

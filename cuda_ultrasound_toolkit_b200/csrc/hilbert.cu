@@ -1,0 +1,196 @@
+// Match-filtered analytic signal, one shared-memory FFT kernel.
+//
+// Upstream (cuda_toolkit/src/rf_processing/rf_ffts/) runs, per frame: a cudaMemset of the
+// output, a strided cuFFT R2C, a mask/scale/filter kernel (hilbert_kernels.cuh:17-40)
+// and an in-place cuFFT C2C inverse (hilbert_handler.cu:132-155). Per row x of N samples:
+//   Y[k] = DFT(x)[k] * w_k * F[k] for k <= N/2, 0 above; w_0 = 0.75/N, w_k = 1.5/N
+//   (the Nyquist bin keeps 1.5/N); F = DFT_N(zero-padded taps), no time reversal
+//   (hilbert_handler.cu:55-78); iq = unnormalised inverse DFT of Y.
+//
+// Here each CTA transforms two rows a, b at once in shared memory and writes the IQ of
+// both exactly once. With G[k] = w_k F[k] (k <= N/2, else 0) split into its Hermitian
+// parts Ge[k] = (G[k] + conj G[-k]) / 2 and Go[k] = (G[k] - conj G[-k]) / (2i), and
+// Z = DFT(x_a + i x_b):
+//   IDFT(Z Ge) = Re(iq_a) + i Re(iq_b),  IDFT(Z Go) = Im(iq_a) + i Im(iq_b),
+// because x_a, x_b are real (their spectra are Hermitian) and so are Ge, Go. That is 1.5
+// complex FFTs per row instead of 2, with no separation step. Ge, Go and the twiddles are
+// precomputed in FP64 on the host and stored as FP32 tables.
+#include <cmath>
+#include <complex>
+#include <vector>
+
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "fft_core.cuh"
+#include "stages.h"
+
+namespace cutb {
+namespace {
+
+using fft::cplx;
+
+template <int LOGN>
+constexpr int hilbert_fft_per_block() { return (1 << LOGN) / 16 >= 128 ? 1 : 128 / ((1 << LOGN) / 16); }
+
+template <int LOGN, int SIGN, int P = 0>
+__device__ __forceinline__ void run_fft(cplx (&x)[16], uint32_t tau, const cplx* tw, float* sre, float* sim)
+{
+    constexpr int NP = fft::pass_count(LOGN);
+    if constexpr (P < NP) {
+        fft::fft_pass<LOGN, P, SIGN>(x, tau, tw, sre, sim);
+        if constexpr (P < NP - 1) {
+            __syncthreads();
+            fft::fft_gather<LOGN>(x, tau, sre, sim);
+            __syncthreads();
+        }
+        run_fft<LOGN, SIGN, P + 1>(x, tau, tw, sre, sim);
+    }
+}
+
+__device__ __forceinline__ void store_iq(float2* out, uint64_t i, float re, float im) { out[i] = make_float2(re, im); }
+__device__ __forceinline__ void store_iq(__nv_bfloat162* out, uint64_t i, float re, float im)
+{
+    out[i] = __floats2bfloat162_rn(re, im);
+}
+
+template <int LOGN, class OutT>
+__global__ void __launch_bounds__(hilbert_fft_per_block<LOGN>() * (1 << LOGN) / 16)
+hilbert_kernel(const float* __restrict__ in, OutT* __restrict__ out, HilbertArgs a)
+{
+    constexpr uint32_t N = 1u << LOGN;
+    constexpr uint32_t TPF = N / 16;
+    constexpr uint32_t FPB = hilbert_fft_per_block<LOGN>();
+    constexpr uint32_t PN = fft::spad_size(N);
+    extern __shared__ float smem[];
+
+    const uint32_t grp = threadIdx.x / TPF, tau = threadIdx.x % TPF;
+    const uint64_t pair = (uint64_t)blockIdx.x * FPB + grp;
+    const uint64_t ra = 2 * pair, rb = ra + 1;
+    const bool has_a = ra < a.rows, has_b = rb < a.rows;
+    float* sre = smem + grp * 2 * PN;
+    float* sim = sre + PN;
+    const cplx* tw = reinterpret_cast<const cplx*>(a.twiddle);
+
+    cplx z[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const uint64_t n = tau + m * TPF;
+        z[m].x = has_a ? __ldcs(in + (ra * N + n) * a.in_stride) : 0.f;
+        z[m].y = has_b ? __ldcs(in + (rb * N + n) * a.in_stride) : 0.f;
+    }
+    run_fft<LOGN, -1>(z, tau, tw, sre, sim);  // z[m] = Z[tau + m*TPF]
+
+    const cplx* ge = reinterpret_cast<const cplx*>(a.ge);
+    const cplx* go = reinterpret_cast<const cplx*>(a.go);
+    cplx r1[16], w[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) r1[m] = fft::cmul(z[m], ge[tau + m * TPF]);
+    __syncthreads();
+    run_fft<LOGN, +1>(r1, tau, tw, sre, sim);
+#pragma unroll
+    for (int m = 0; m < 16; ++m) w[m] = fft::cmul(z[m], go[tau + m * TPF]);
+    __syncthreads();
+    run_fft<LOGN, +1>(w, tau, tw, sre, sim);
+
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const uint64_t n = tau + m * TPF;
+        if (has_a) store_iq(out, ra * N + n, r1[m].x, w[m].x);
+        if (has_b) store_iq(out, rb * N + n, r1[m].y, w[m].y);
+    }
+}
+
+template <int LOGN, class OutT>
+bool launch_hilbert_t(const float* in, void* out, const HilbertArgs& a, cudaStream_t st)
+{
+    constexpr uint32_t N = 1u << LOGN;
+    constexpr uint32_t FPB = hilbert_fft_per_block<LOGN>();
+    const size_t smem = (size_t)FPB * 2 * fft::spad_size(N) * sizeof(float);
+    auto kern = hilbert_kernel<LOGN, OutT>;
+    static bool configured = false;
+    if (!configured) {
+        CUTB_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = true;
+    }
+    const uint64_t pairs = (a.rows + 1) / 2;
+    const uint64_t blocks = div_up(pairs, (uint64_t)FPB);
+    CUTB_REQUIRE(blocks <= 0x7fffffffull, CUTB_ERR_INVALID_ARGUMENT, "Too many rows for one launch.");
+    kern<<<(unsigned)blocks, FPB * (N / 16), smem, st>>>(in, (OutT*)out, a);
+    CUTB_CUDA_OK(cudaGetLastError());
+    return true;
+}
+
+template <class OutT>
+bool launch_hilbert_o(const float* in, void* out, const HilbertArgs& a, cudaStream_t st)
+{
+    switch (a.log_n) {
+        case 4: return launch_hilbert_t<4, OutT>(in, out, a, st);
+        case 5: return launch_hilbert_t<5, OutT>(in, out, a, st);
+        case 6: return launch_hilbert_t<6, OutT>(in, out, a, st);
+        case 7: return launch_hilbert_t<7, OutT>(in, out, a, st);
+        case 8: return launch_hilbert_t<8, OutT>(in, out, a, st);
+        case 9: return launch_hilbert_t<9, OutT>(in, out, a, st);
+        case 10: return launch_hilbert_t<10, OutT>(in, out, a, st);
+        case 11: return launch_hilbert_t<11, OutT>(in, out, a, st);
+        case 12: return launch_hilbert_t<12, OutT>(in, out, a, st);
+        case 13: return launch_hilbert_t<13, OutT>(in, out, a, st);
+        case 14: return launch_hilbert_t<14, OutT>(in, out, a, st);
+        default: break;
+    }
+    set_error(CUTB_ERR_UNSUPPORTED, "Hilbert transform length 2^%u not supported.", a.log_n);
+    return false;
+}
+
+}  // namespace
+
+bool hilbert_supported_length(unsigned n) { return is_pow2(n) && n >= 16 && n <= kMaxHilbertLength; }
+
+// Host tables: twiddles exp(-2*pi*i*m/N) and the Hermitian parts of the spectral weight
+// G = w * F, all computed in double and rounded once to float.
+bool build_hilbert_tables(unsigned n, const float* taps, unsigned ntaps, std::vector<float>& twiddle,
+                          std::vector<float>& ge, std::vector<float>& go)
+{
+    CUTB_REQUIRE(hilbert_supported_length(n), CUTB_ERR_UNSUPPORTED,
+                 "Sample count %u not supported by the FFT (powers of two 16..%u).", n, kMaxHilbertLength);
+    CUTB_REQUIRE(ntaps <= n, CUTB_ERR_INVALID_ARGUMENT, "Match filter longer (%u) than the sample count (%u).", ntaps,
+                 n);
+    using cd = std::complex<double>;
+    const double two_pi = 6.283185307179586476925286766559;
+    twiddle.resize(2 * (size_t)n);
+    std::vector<cd> root(n);
+    for (unsigned m = 0; m < n; ++m) {
+        root[m] = std::polar(1.0, -two_pi * (double)m / (double)n);
+        twiddle[2 * m] = (float)root[m].real();
+        twiddle[2 * m + 1] = (float)root[m].imag();
+    }
+    std::vector<cd> g(n, cd(0, 0));
+    const unsigned half = n / 2;
+    for (unsigned k = 0; k <= half; ++k) {
+        cd f(1.0, 0.0);
+        if (ntaps) {
+            f = 0;
+            for (unsigned t = 0; t < ntaps; ++t) f += (double)taps[t] * root[(uint64_t)k * t % n];
+        }
+        g[k] = ((k == 0 ? 0.75 : 1.5) / (double)n) * f;
+    }
+    ge.resize(2 * (size_t)n);
+    go.resize(2 * (size_t)n);
+    for (unsigned k = 0; k < n; ++k) {
+        const cd gm = std::conj(g[(n - k) % n]);
+        const cd e = 0.5 * (g[k] + gm);
+        const cd o = (g[k] - gm) / cd(0.0, 2.0);
+        ge[2 * k] = (float)e.real();
+        ge[2 * k + 1] = (float)e.imag();
+        go[2 * k] = (float)o.real();
+        go[2 * k + 1] = (float)o.imag();
+    }
+    return true;
+}
+
+bool launch_hilbert(const HilbertArgs& a, const float* in, void* out, bool bf16, cudaStream_t st)
+{
+    return bf16 ? launch_hilbert_o<__nv_bfloat162>(in, out, a, st) : launch_hilbert_o<float2>(in, out, a, st);
+}
+
+}  // namespace cutb

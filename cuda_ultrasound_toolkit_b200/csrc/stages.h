@@ -1,0 +1,79 @@
+// Internal interfaces between the plan (plan.cu) and the stage kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <vector>
+
+#include "../../include/cuda_beamformer_parameters.h"
+
+namespace cutb {
+
+// ---- convert + reorder + decode (decode.cu) ------------------------------------------
+struct DecodeArgs {
+    uint64_t R0;               // raw row length in elements (samples*transmits + padding)
+    uint32_t S, C, T;          // samples, receive channels, transmits
+    uint32_t L, G;             // transmit lanes per sample group, sample groups per warp (32 / L)
+    const int16_t* map;        // device: raw channel of each receive channel (C entries)
+    const uint16_t* out_row;   // device: natural decode row -> output row (T entries)
+    float alpha;               // fl32(1 / T), or 1 when not decoding
+};
+
+struct DecodeSetup {
+    DecodeArgs args{};
+    int encoding = NONE;       // NONE, HADAMARD or WALSH
+    unsigned base = 1, R = 1;  // base matrix order, transmits held in registers
+};
+
+bool plan_decode_split(unsigned T, unsigned base, unsigned& R, unsigned& L);
+bool launch_decode(const DecodeSetup& d, const void* raw, int data_type, float* out, unsigned out_stride,
+                   cudaStream_t st);
+
+// ---- analytic signal (hilbert.cu) --------------------------------------------------------
+constexpr unsigned kMaxHilbertLength = 16384;
+
+struct HilbertArgs {
+    uint64_t rows;             // T * C rows of N samples
+    uint32_t log_n;            // N = 2^log_n
+    uint32_t in_stride;        // 1: packed floats, 2: real part of complex input
+    const float* twiddle;      // device: N complex exp(-2 pi i m / N)
+    const float* ge;           // device: N complex, Hermitian-even part of the spectral weight
+    const float* go;           // device: N complex, Hermitian-odd part (divided by i)
+};
+
+bool hilbert_supported_length(unsigned n);
+bool build_hilbert_tables(unsigned n, const float* taps, unsigned ntaps, std::vector<float>& twiddle,
+                          std::vector<float>& ge, std::vector<float>& go);
+bool launch_hilbert(const HilbertArgs& a, const float* in, void* out, bool bf16, cudaStream_t st);
+
+// ---- delay and sum (das.cu) ----------------------------------------------------------------
+struct DasArgs {
+    int S, C, T, G;            // samples, channels, transmits, READI sub-signals (>= 1)
+    int X, Y, Z;               // output grid
+    int seq;                   // HERCULES or FORCES
+    int focus;                 // YZ_PLANE (2) or YZ_FOCUS (4) for HERCULES
+    int encoding;              // READI sub-signal ordering: HADAMARD or WALSH
+    int cubic;                 // 1: Catmull-Rom, 0: linear
+    int apo_type;              // ApoType
+    int use_apo;               // 0: every apodization weight is exactly 1
+    int apply_cf;              // multiply by the coherence factor
+    float spm;                 // samples per metre, fs / c
+    float px, py;              // element pitch
+    float xmin_x, xmin_y;      // first element centre
+    float xmax_x, xmax_y;      // last element centre
+    float delay;               // (int)(time_offset * fs)
+    float vmin_x, vmin_y, vmin_z;
+    float res_x, res_y, res_z;
+    float fz;                  // focal depth (0 for plane waves)
+    float fn_rx, fn_tx;
+    float cf_power;            // coherence exponent in [0, 1]
+    float to_power;            // sine apodization exponent
+    unsigned long long readi_row;  // bit g set: sub-signal g negated
+};
+
+// Derives the delay-and-sum constants from the parameter block, applying the same
+// validation as the upstream dispatcher (beamformer.cu:17-197).
+bool derive_das(const CudaBeamformerParameters& bp, DasArgs& a);
+bool launch_das(const DasArgs& a, const void* iq, bool iq_bf16, void* volume, cudaStream_t st, int* launches);
+
+}  // namespace cutb

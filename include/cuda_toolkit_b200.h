@@ -1,0 +1,112 @@
+/*
+ * Device-resident API of the B200 RF -> volume library.
+ *
+ * The upstream toolkit exposes only host-span entry points (cuda_toolkit::beamform,
+ * the MATLAB wrappers) and a GL-buffer front end. Its internal stages are the
+ * classes RfProcessor (cuda_toolkit/src/rf_processing/rf_processor.cpp:20-192) and
+ * Beamformer (cuda_toolkit/src/beamformer/beamformer.cu:17-197). This header exposes
+ * the same stages on caller-owned device memory and a caller-chosen CUDA stream, so
+ * they can be timed, captured in a CUDA graph and checked stage by stage:
+ *
+ *   cutb_decode   <- RfProcessor::convert_decode_strided / convert_strided (rf_processor.cpp:118-173)
+ *   cutb_hilbert  <- RfProcessor::hilbert_transform_strided (rf_processor.cpp:175-192)
+ *   cutb_das      <- Beamformer::beamform (beamformer.cu:139-197)
+ *   cutb_beamform <- the stage sequence of cuda_toolkit::beamform (cuda_toolkit.cpp:153-186)
+ *
+ * All pointers are plain device pointers; `stream` is a cudaStream_t (NULL = legacy
+ * default stream). Calls are asynchronous with respect to the host unless noted.
+ * Every function returns false (or NULL / 0) on error, logs one line to stderr
+ * (silence with CUTB_LOG=0) and records a code readable with cutb_last_error().
+ */
+#ifndef CUDA_TOOLKIT_B200_H
+#define CUDA_TOOLKIT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "cuda_beamformer_parameters.h"
+
+#if defined(_WIN32)
+#define CUTB_API __declspec(dllexport)
+#else
+#define CUTB_API __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error codes returned by cutb_last_error(). */
+enum {
+    CUTB_OK = 0,
+    CUTB_ERR_INVALID_ARGUMENT = 1, /* bad pointer, size or dimension */
+    CUTB_ERR_UNSUPPORTED = 2,      /* valid upstream value that this path does not run */
+    CUTB_ERR_NOT_INITIALIZED = 3,  /* call order violated (e.g. decode before init) */
+    CUTB_ERR_CUDA = 4,             /* a CUDA runtime call failed */
+    CUTB_ERR_ALLOCATION = 5,       /* device allocation failed (or injected failure) */
+    CUTB_ERR_TIMEOUT = 6,          /* a bounded device-side wait gave up */
+};
+
+/* Code and message of the most recent failure on the calling thread. */
+CUTB_API int cutb_last_error(void);
+CUTB_API const char* cutb_last_error_message(void);
+CUTB_API void cutb_clear_error(void);
+
+/* Library version, (major << 16) | minor. */
+CUTB_API int cutb_version(void);
+
+/* Encoding matrix of order n as generated upstream (hadamard_decoder.cpp:110-222):
+ * row-major +1/-1 bytes, ordering HADAMARD (1) or WALSH (2). n = 2^k, 12*2^k or 20*2^k, n <= 1024. */
+CUTB_API bool cutb_encoding_matrix(uint n, int ordering, signed char* out);
+
+/* Options that the parameter struct has no field for. Zero-initialise for defaults. */
+typedef struct cutb_options {
+    int iq_bf16;      /* 1: analytic signal stored as bf16 complex (halves DAS gather bytes) */
+    int das_tile;     /* 0: tuned/default tile; >0: explicit tile id (autotuner) */
+    int reserved[14];
+} cutb_options;
+
+typedef struct cutb_plan cutb_plan;
+
+/* Validates bp and prepares everything that depends only on it: the decode transform,
+ * the channel map, the match-filter spectrum, the delay-and-sum constants and the
+ * intermediate device buffers. Synchronous. */
+CUTB_API cutb_plan* cutb_plan_create(const CudaBeamformerParameters* bp, const cutb_options* options);
+CUTB_API void cutb_plan_destroy(cutb_plan* plan);
+
+/* Byte sizes of the raw input, one analytic-signal buffer [T][C][S] and the output volume [Z][Y][X]. */
+CUTB_API size_t cutb_plan_raw_bytes(const cutb_plan* plan);
+CUTB_API size_t cutb_plan_iq_bytes(const cutb_plan* plan);
+CUTB_API size_t cutb_plan_volume_bytes(const cutb_plan* plan);
+
+/* Convert + reorder + decode: d_raw [R1][R0] (int16 or f32) -> d_out f32 [T][C][S].
+ * out_stride 1 writes packed floats; 2 writes complex [T][C][S] with .y = 0. */
+CUTB_API bool cutb_decode(cutb_plan* plan, const void* d_raw, size_t raw_bytes, float* d_out, uint out_stride,
+                          void* stream);
+
+/* Match-filtered analytic signal of every [T][C] row: d_in f32 with element stride in_stride
+ * (1 = packed, 2 = real part of complex) -> d_iq complex [T][C][S] (complex64, or bf16x2
+ * when the plan stores bf16). */
+CUTB_API bool cutb_hilbert(cutb_plan* plan, const float* d_in, uint in_stride, void* d_iq, void* stream);
+
+/* Delay-and-sum of d_iq [T][C][S] into the complex64 volume d_volume [Z][Y][X]. */
+CUTB_API bool cutb_das(cutb_plan* plan, const void* d_iq, void* d_volume, void* stream);
+
+/* Whole pipeline on device memory, intermediates in the plan's own buffers. */
+CUTB_API bool cutb_beamform(cutb_plan* plan, const void* d_raw, size_t raw_bytes, void* d_volume, void* stream);
+
+/* Number of kernels the last cutb_beamform/cutb_decode/cutb_hilbert/cutb_das call launched. */
+CUTB_API int cutb_plan_last_launch_count(const cutb_plan* plan);
+
+/* Measures the device's FP32 fused-multiply-add throughput (TFLOP/s) with a short
+ * register-only kernel on `stream`; the roofline denominator of the delay-and-sum stage. */
+CUTB_API bool cutb_calibrate_fp32(double* tflops, void* stream);
+
+/* Test hook: the next `after` device allocations succeed, then allocations fail until
+ * reset with a negative value. Used to exercise the allocation-failure paths. */
+CUTB_API void cutb_debug_fail_allocations_after(int after);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUDA_TOOLKIT_B200_H */

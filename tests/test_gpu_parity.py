@@ -1,0 +1,329 @@
+"""Parity of the CUDA path (through the C ABI) against the CPU oracle.
+
+Bars: the convert + reorder + decode stage is bit-exact against the oracle's exact
+restatement of the upstream FP32 result; the analytic signal and the volume are compared
+with the FP64 oracle by relative L2 error (tolerances stated per test).
+"""
+import ctypes
+import math
+
+import numpy as np
+import pytest
+
+from cuda_ultrasound_toolkit_b200 import (ApoType, CutbError, EncodingMatrix, InputDataTypes, Plan, RfSession,
+                                          SequenceId, beamform, beamform_f32, beamform_i16, synth)
+from cuda_ultrasound_toolkit_b200.params import CudaBeamformerParameters
+
+pytestmark = pytest.mark.gpu
+
+# Relative L2 tolerances (GPU FP32 vs oracle FP64).
+TOL_HILBERT = 2e-6          # FP32 shared-memory FFT, twiddles rounded once from FP64
+TOL_DAS_RANDOM = 2e-4       # random analytic rows: FP32 delay rounding (~1e-4 sample) x signal slope
+TOL_DAS_APO = 2e-3          # Hann / sine apodization in FP32 (__cosf, sinf) and 0.1-threshold flips
+TOL_VOLUME = 1e-5           # phantom volume (coherent sum) through the whole pipeline
+
+
+def rel_l2(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    assert t.cuda.is_available()
+    return t
+
+
+def base_params(S, C, T, X=16, Y=8, Z=24, R0=None, R1=None, decode=EncodingMatrix.HADAMARD, cmap=None,
+                data_type=InputDataTypes.TYPE_I16):
+    w = synth.Workload("t", T, C, S, X, Y, Z, 0, cubic=True, cf=0.0, encoding=decode)
+    bp = synth.make_params(w, data_type=data_type, channel_map=cmap)
+    if R0 is not None:
+        bp.rf_raw_dim[0] = R0
+    if R1 is not None:
+        bp.rf_raw_dim[1] = R1
+    return bp
+
+
+# ---------------------------------------------------------------------------------------------
+# convert + reorder + decode
+# ---------------------------------------------------------------------------------------------
+DECODE_CASES = [
+    # (T, ordering, S, C, padding, extra raw channels)
+    (1, 1, 64, 3, 0, 0), (2, 1, 64, 3, 0, 0), (8, 2, 64, 5, 7, 2), (16, 1, 128, 4, 0, 0), (32, 2, 64, 3, 0, 1),
+    (64, 1, 256, 6, 0, 0), (128, 1, 64, 4, 16, 3), (128, 2, 64, 4, 0, 0), (256, 1, 32, 3, 0, 0),
+    (512, 2, 32, 2, 0, 0), (1024, 1, 16, 2, 0, 0),
+    (12, 1, 64, 3, 0, 0), (24, 2, 64, 3, 4, 1), (96, 1, 32, 3, 0, 0), (768, 1, 16, 2, 0, 0),
+    (20, 1, 64, 3, 0, 0), (40, 2, 32, 3, 0, 0), (640, 1, 16, 2, 0, 0),
+    (64, 0, 64, 4, 3, 1),  # decode == NONE
+    (16, 1, 34, 3, 0, 0),  # sample count not a multiple of 4: scalar-load path
+    (20, 1, 30, 3, 1, 0),  # idem for the base-20 kernel
+]
+
+
+@pytest.mark.parametrize("T,ordering,S,C,pad,extra", DECODE_CASES)
+@pytest.mark.parametrize("out_stride", [1, 2])
+def test_decode_bit_exact_int16(torch, orc, T, ordering, S, C, pad, extra, out_stride):
+    rng = np.random.default_rng(T * 1000 + S + ordering)
+    R0, R1 = T * S + pad, C + extra
+    raw = rng.integers(-32768, 32768, size=(R1, R0), dtype=np.int16)
+    cmap = rng.permutation(R1)[:C]
+    bp = base_params(S, C, T, R0=R0, R1=R1, decode=ordering, cmap=cmap)
+    plan = Plan(bp)
+    out = plan.decode(torch.from_numpy(raw).cuda(), out_stride=out_stride)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().reshape(T, C, S, out_stride)
+    ref = orc.decode_i16(raw, bp)
+    assert np.array_equal(got[..., 0], ref)
+    if out_stride == 2:
+        assert not got[..., 1].any()
+    assert plan.launches == 1
+
+
+def test_decode_f32_integer_valued_bit_exact(torch, orc):
+    rng = np.random.default_rng(2)
+    S, C, T = 256, 8, 128
+    raw16 = rng.integers(-32768, 32768, size=(C, T * S), dtype=np.int16)
+    bp = base_params(S, C, T, cmap=rng.permutation(C), data_type=InputDataTypes.TYPE_F32)
+    got = Plan(bp).decode(torch.from_numpy(raw16.astype(np.float32)).cuda()).cpu().numpy()
+    assert np.array_equal(got, orc.decode_i16(raw16, bp))
+
+
+def test_decode_f32_general(torch, orc):
+    rng = np.random.default_rng(3)
+    S, C, T = 128, 4, 96
+    raw = rng.normal(size=(C, T * S)).astype(np.float32)
+    bp = base_params(S, C, T, cmap=rng.permutation(C), data_type=InputDataTypes.TYPE_F32)
+    got = Plan(bp).decode(torch.from_numpy(raw).cuda()).cpu().numpy()
+    assert rel_l2(got, orc.decode_f64(raw, bp)) < 1e-6
+
+
+# ---------------------------------------------------------------------------------------------
+# Hilbert
+# ---------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("N", [16, 64, 256, 1024, 2048, 4096, 8192])
+@pytest.mark.parametrize("taps", [0, 64])
+def test_hilbert_vs_fp64(torch, orc, N, taps):
+    T, C = 3, 5                                    # 15 rows: odd count exercises the unpaired row
+    rng = np.random.default_rng(N + taps)
+    rows = rng.normal(size=(T, C, N)).astype(np.float32)
+    bp = base_params(N, C, T)
+    h = None
+    if taps:
+        h = synth.chirp_taps(min(taps, N))
+        bp.filter_length = len(h)
+        for i, v in enumerate(h):
+            bp.rf_filter[i] = float(v)
+    plan = Plan(bp)
+    got = plan.hilbert(torch.from_numpy(rows).cuda()).cpu().numpy()
+    ref = orc.hilbert(rows.astype(np.float64), h)
+    assert rel_l2(got, ref) < TOL_HILBERT
+
+
+def test_hilbert_strided_input_and_known_answer(torch, orc):
+    N, T, C = 1024, 2, 2
+    n = np.arange(N)
+    rows = np.stack([np.cos(2 * np.pi * k * n / N) for k in (1, 5, 100, N // 2)]).reshape(T, C, N)
+    cplx = np.zeros((T, C, N, 2), np.float32)
+    cplx[..., 0] = rows
+    cplx[..., 1] = 123.0                           # the imaginary part must be ignored
+    plan = Plan(base_params(N, C, T))
+    got = plan.hilbert(torch.from_numpy(cplx).cuda().reshape(T, C, 2 * N), in_stride=2).cpu().numpy()
+    expect = np.stack([0.75 * np.exp(2j * np.pi * k * n / N) for k in (1, 5, 100)] + [1.5 * (-1.0) ** n])
+    np.testing.assert_allclose(got.reshape(4, N), expect, atol=2e-6)
+
+
+# ---------------------------------------------------------------------------------------------
+# delay and sum
+# ---------------------------------------------------------------------------------------------
+def das_params(seq=SequenceId.HERCULES, cubic=True, cf=0.0, fn_rx=0.0, fn_tx=0.0, apo=ApoType.RX_HANN,
+               readi=0, readi_id=0, decode=EncodingMatrix.HADAMARD, focus_z=math.inf, S=512, C=8, T=8,
+               X=20, Y=9, Z=40, z=(4e-3, 26e-3), time_offset=0.0):
+    bp = base_params(S, C, T, X=X, Y=Y, Z=Z, decode=decode)
+    bp.das_shader_id = int(seq)
+    bp.interpolate = bool(cubic)
+    bp.coherency_weighting = cf
+    bp.fn_rx, bp.fn_tx = fn_rx, fn_tx
+    bp.apo_type = int(apo)
+    bp.to_power = 2
+    bp.readi_group_count, bp.readi_group_id = readi, readi_id
+    bp.foci[2] = focus_z
+    bp.output_min_coordinate[0], bp.output_max_coordinate[0] = -3e-3, 3e-3
+    bp.output_min_coordinate[1] = -1e-3
+    bp.output_min_coordinate[2], bp.output_max_coordinate[2] = z
+    bp.time_offset = time_offset
+    return bp
+
+
+def analytic_rows(orc, T, C, S, seed):
+    """Band-limited analytic rows (Hilbert of random pulses), the kind of data DAS sees."""
+    rng = np.random.default_rng(seed)
+    x = np.zeros((T, C, S))
+    n = np.arange(S)
+    for _ in range(12):
+        c0 = rng.uniform(20, S - 20)
+        x += rng.normal() * np.exp(-0.5 * ((n - c0) / 3.4) ** 2) * np.cos(2 * np.pi * 0.25 * (n - c0))
+    x += 0.05 * rng.normal(size=x.shape)
+    return orc.hilbert(x)
+
+
+DAS_CASES = [
+    dict(),                                             # HERCULES plane wave, cubic, no CF
+    dict(cubic=False),
+    dict(cf=1.0),
+    dict(cf=0.5, cubic=False),
+    dict(focus_z=15e-3),                                # YZ_FOCUS
+    dict(time_offset=2e-7),
+    dict(z=(0.0, 60e-3)),                               # reaches z = 0 and the clamp at S-2
+    dict(readi=2, readi_id=1),
+    dict(readi=4, readi_id=2, decode=EncodingMatrix.WALSH),
+    dict(seq=SequenceId.FORCES),
+    dict(seq=SequenceId.FORCES, cubic=False, cf=0.3),
+    dict(seq=SequenceId.FORCES, readi=2, readi_id=1),
+    dict(X=33, Y=3, Z=70),                              # partial tiles in every direction
+]
+DAS_APO_CASES = [
+    dict(fn_rx=1.5),
+    dict(apo=ApoType.RX_TO_SIN),
+    dict(seq=SequenceId.FORCES, fn_rx=1.0, fn_tx=2.0),
+    dict(seq=SequenceId.FORCES, apo=ApoType.RX_TO_SIN),
+    dict(seq=SequenceId.FORCES, apo=ApoType.TX_TO_SIN),
+    dict(seq=SequenceId.FORCES, apo=ApoType.BOTH_TO_SIN),
+]
+
+
+@pytest.mark.parametrize("case", DAS_CASES + DAS_APO_CASES, ids=lambda c: ",".join(f"{k}={v}" for k, v in c.items()) or "default")
+def test_das_vs_fp64(torch, orc, case):
+    bp = das_params(**case)
+    S, C, T = bp.dims
+    iq = analytic_rows(orc, T, C, S, seed=len(str(case)))
+    plan = Plan(bp)
+    got = plan.das(torch.from_numpy(iq.astype(np.complex64)).cuda()).cpu().numpy()
+    ref = orc.das(iq, bp)
+    tol = TOL_DAS_APO if case in DAS_APO_CASES else TOL_DAS_RANDOM
+    err = rel_l2(got, ref)
+    assert err < tol, err
+    if bp.das_shader_id == SequenceId.FORCES:      # y-invariant
+        assert (got == got[:, :1, :]).all()
+
+
+def test_das_bf16_storage(torch, orc):
+    bp = das_params(cf=1.0)
+    S, C, T = bp.dims
+    iq = analytic_rows(orc, T, C, S, seed=9)
+    plan = Plan(bp, iq_bf16=True)
+    iq_b = torch.from_numpy(np.stack([iq.real, iq.imag], -1).astype(np.float32)).cuda().to(torch.bfloat16)
+    got = plan.das(iq_b).cpu().numpy()
+    assert rel_l2(got, orc.das(iq, bp)) < 2e-2     # bf16 keeps 8 bits of mantissa
+
+
+# ---------------------------------------------------------------------------------------------
+# whole pipeline
+# ---------------------------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def small_frame():
+    return synth.frame("small")
+
+
+def test_pipeline_small_vs_oracle(torch, orc, small_frame):
+    raw, bp = small_frame
+    plan = Plan(bp)
+    d_raw = torch.from_numpy(raw).cuda()
+    vol = plan.beamform(d_raw).cpu().numpy()
+    assert plan.launches == 3
+    dec = plan.decode(d_raw).cpu().numpy()
+    assert np.array_equal(dec, orc.decode_i16(raw, bp))
+    iq = plan.hilbert(torch.from_numpy(dec).cuda()).cpu().numpy()
+    iq_ref = orc.hilbert(dec.astype(np.float64))
+    assert rel_l2(iq, iq_ref) < TOL_HILBERT
+    rng = np.random.default_rng(0)
+    vox = rng.choice(vol.size, 4096, replace=False)
+    ref = orc.das(iq_ref, bp, vox)
+    assert rel_l2(vol.ravel()[vox], ref) < TOL_VOLUME
+
+
+def test_host_span_entry_points(torch, small_frame):
+    raw, bp = small_frame
+    ref = Plan(bp).beamform(torch.from_numpy(raw).cuda()).cpu().numpy()
+    assert np.array_equal(beamform(raw, bp), ref)
+    assert np.array_equal(beamform_i16(raw, bp), ref)
+    bpf = bp.copy()
+    bpf.data_type = InputDataTypes.TYPE_F32
+    assert np.array_equal(beamform_f32(raw.astype(np.float32), bpf), ref)
+    with pytest.raises(CutbError):                  # output span too short
+        beamform(raw, bp, out=np.empty(10, np.complex64))
+
+
+def test_buffer_registry_front_end(torch, orc, small_frame):
+    raw, bp = small_frame
+    S, C, T = bp.dims
+    sess = RfSession((int(bp.rf_raw_dim[0]), int(bp.rf_raw_dim[1])), (S, C, T))
+    try:
+        pad = 64                                            # input offset into the raw buffer
+        d_raw = torch.zeros(raw.size + pad // 2, dtype=torch.int16, device="cuda")
+        d_raw[pad // 2:] = torch.from_numpy(raw.ravel()).cuda()
+        bufs = [torch.full((T, C, S), 7 + 7j, dtype=torch.complex64, device="cuda") for _ in range(2)]
+        raw_id = sess.register(d_raw)
+        ids = [sess.register(b) for b in bufs]
+        sess.register_buffers(ids, raw_id)
+        sess.set_channel_mapping(np.ctypeslib.as_array(bp.channel_mapping)[:C])
+        taps = synth.chirp_taps(32)
+        sess.set_match_filter(taps)
+        sess.decode(pad, 0)
+        dec = bufs[0].cpu().numpy()
+        ref = orc.decode_i16(raw, bp)
+        assert np.array_equal(dec.real, ref) and not dec.imag.any()
+        sess.hilbert(0, 1)
+        iq = bufs[1].cpu().numpy()
+        assert rel_l2(iq, orc.hilbert(ref.astype(np.float64), taps)) < TOL_HILBERT
+        with pytest.raises(CutbError):
+            sess.decode(0, 5)                               # index beyond the registered buffers
+    finally:
+        sess.close()
+
+
+# ---------------------------------------------------------------------------------------------
+# error contract
+# ---------------------------------------------------------------------------------------------
+def test_invalid_parameters_are_rejected(torch):
+    S, C, T = 64, 4, 8
+    bad = []
+    bp = base_params(S, C, T, R0=T * S - 1); bad.append((bp, 1))               # rows shorter than T*S
+    bp = base_params(S, C, 36); bad.append((bp, 2))                             # unsupported order
+    bp = base_params(S, C, T); bp.channel_mapping[1] = 99; bad.append((bp, 1))  # map outside raw channels
+    bp = base_params(S, C, T); bp.sample_type = 1; bad.append((bp, 2))          # bandpass input
+    bp = base_params(S, C, T); bp.data_type = 4; bad.append((bp, 2))            # u8 input
+    bp = base_params(S, C, T); bp.das_shader_id = SequenceId.RCA_VLS; bad.append((bp, 2))
+    bp = base_params(S, C, T); bp.rx_orientation = bp.tx_orientation; bad.append((bp, 2))  # XZ focus for HERCULES
+    bp = base_params(S, C, T); bp.readi_group_count = 2; bp.readi_group_id = 5; bad.append((bp, 1))
+    bp = base_params(S, C, T); bp.filter_length = S + 1; bad.append((bp, 1))
+    for bp, code in bad:
+        with pytest.raises(CutbError) as e:
+            Plan(bp)
+        assert e.value.code == code, e.value
+    plan = Plan(base_params(100, C, T))              # decode works, the FFT length does not
+    with pytest.raises(CutbError) as e:
+        plan.beamform(torch.zeros(100 * T * C, dtype=torch.int16, device="cuda"))
+    assert e.value.code == 2
+
+
+def test_allocation_failure_injection(torch):
+    from cuda_ultrasound_toolkit_b200 import lib
+    bp = base_params(64, 4, 8)
+    lib().cutb_debug_fail_allocations_after(1)
+    try:
+        with pytest.raises(CutbError) as e:
+            Plan(bp)
+        assert e.value.code == 5
+    finally:
+        lib().cutb_debug_fail_allocations_after(-1)
+    Plan(bp)
+
+
+def test_short_raw_buffer_rejected(torch):
+    bp = base_params(64, 4, 8)
+    plan = Plan(bp)
+    with pytest.raises(CutbError):
+        plan.beamform(torch.zeros(10, dtype=torch.int16, device="cuda"))
