@@ -65,6 +65,7 @@ def lib():
         "cutb_beamform": ([vp, vp, sz, vp, vp], b),
         "cutb_debug_fail_allocations_after": ([ctypes.c_int], None),
         "cutb_calibrate_fp32": ([ctypes.POINTER(ctypes.c_double), vp], b),
+        "cutb_plan_check": ([vp, vp], b),
         "init_cuda_configuration": ([ctypes.POINTER(u), ctypes.POINTER(u)], b),
         "register_cuda_buffers": ([ctypes.POINTER(u), u, u], b),
         "cuda_set_channel_mapping": ([ctypes.POINTER(ctypes.c_int16)], b),
@@ -224,6 +225,10 @@ class Plan:
         out = self.empty_volume() if out is None else out
         _check(lib().cutb_das(self._h, iq.data_ptr(), out.data_ptr(), _stream_handle(stream)), "cutb_das")
         return out
+
+    def check(self, stream=None):
+        """Synchronises the stream; raises if a device-side bounded wait gave up."""
+        _check(lib().cutb_plan_check(self._h, _stream_handle(stream)), "cutb_plan_check")
 
     def beamform(self, raw, out=None, stream=None):
         out = self.empty_volume() if out is None else out

@@ -91,7 +91,7 @@ bool beamform_impl(const uint8_t* in, size_t in_size, uint8_t* out, size_t out_s
     CUTB_CUDA_OK(cudaMemcpy(st.d_input, in, p->raw_bytes, cudaMemcpyHostToDevice));  // cuda_toolkit.cpp:132
     if (!cutb_beamform(p, st.d_input, p->raw_bytes, st.d_output, nullptr)) return false;
     CUTB_CUDA_OK(cudaMemcpy(out, st.d_output, p->vol_bytes, cudaMemcpyDeviceToHost));  // cuda_toolkit.cpp:188
-    return true;
+    return cutb_plan_check(p, nullptr);
 }
 
 // ---- buffer-registry session (upstream cuda_toolkit_ogl.cpp:5-30) ---------------------------------

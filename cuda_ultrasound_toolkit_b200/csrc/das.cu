@@ -7,12 +7,20 @@
 // with the constants of Beamformer::_params_to_constants (beamformer.cu:17-98) and the
 // dispatch rules of Beamformer::beamform (beamformer.cu:139-197, 223-413).
 //
-// Design: a CTA owns a tile of voxels and walks the [T][C] analytic-signal rows. For
-// each row it stages only the window of samples that the tile can address (computed by
-// interval arithmetic on the delay over the tile's bounding box) into shared memory, so
-// the four-tap gathers of every voxel hit shared memory instead of L1/L2. Lanes of a warp
-// are consecutive depths, whose delays differ by a few samples, which keeps the gathers
-// free of bank conflicts. Delays are computed on the fly in FP32 from per-voxel bases.
+// Design. A CTA owns a tile of 4 x 8 x 32 voxels (x, y, z; FORCES: 32 x 1 x 32) and walks
+// the analytic-signal rows (t, c) in stages of 16 channels. For every row of a stage, one
+// lane of warp 0 computes the window of samples the tile can address and issues a TMA bulk
+// copy (cp.async.bulk) of exactly that window into shared memory; three stage buffers
+// with mbarrier completion keep two stages of copies in flight while all warps
+// interpolate from shared memory. Lanes of a warp are consecutive depths, whose delays
+// differ by a few samples, so the four-tap gathers do not conflict on banks.
+//
+// Delays are formed relative to an FP64 origin at the tile centre: per row the FP64
+// distance d0 from the tile centre to the element gives the absolute sample index of the
+// centre; per voxel (offset delta from the centre, exact in FP32) the FP32 correction
+// d - d0 = (d^2 - d0^2) / (d + d0) with d^2 - d0^2 = -2 (e - centre).delta + |delta|^2 keeps
+// the index error near 1e-5 samples, instead of ~1e-4 for a direct FP32 sqrt of the
+// ~5 cm path length.
 //
 // Choices where upstream is silent or self-contradictory (documented for users):
 //   * interpolate == false -> linear, true -> cubic Catmull-Rom (upstream always cubic);
@@ -32,34 +40,74 @@
 namespace cutb {
 namespace {
 
-constexpr int kDasThreads = 256;
-constexpr int kVpt = 4;          // voxels per thread (along x)
-constexpr int kCps = 8;          // channel rows staged per step
-constexpr int kWinMax = 256;     // samples per staged window
-constexpr int kWinStride = kWinMax + 4;
+constexpr int kThreads = 128;
+constexpr int kWarps = kThreads / 32;
+constexpr int kVpt = 8;           // voxels per thread (along z)
+constexpr int kRows = 8;          // rows (channels) per stage
+constexpr int kStages = 3;        // raw stage buffers in flight
+constexpr int kWinMax = 136;      // samples per staged window
+constexpr int kBatch = 8;         // stages whose window metadata is computed together
 constexpr float kPi = 3.141592654f;  // value of CUDART_PI_F used upstream
+constexpr long long kWaitLimitCycles = 400000000ll;  // ~0.2 s at 2 GHz
 
-struct Interval {
-    float lo, hi;
-};
+// ---- PTX helpers: mbarrier + bulk copy (TMA) ----------------------------------------------
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ Interval sq_range(float a, float b)
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
 {
-    const float lo = (a <= 0.f && b >= 0.f) ? 0.f : fminf(a * a, b * b);
-    return {lo, fmaxf(a * a, b * b)};
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
 }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: false if the phase did not complete within kWaitLimitCycles.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long start = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - start > kWaitLimitCycles) return false;
+    return true;
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
-__device__ __forceinline__ float fast_sqrt(float x)
+__device__ __forceinline__ float approx_sqrt(float x)
 {
     float r;
     asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float approx_rcp(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
 
 // f-number Hann window, beamformer_utils.cuh:142-154.
 __device__ __forceinline__ float hann_apo(float lateral, float depth, float fnum)
 {
-    float a = fminf(fnum * (lateral / depth) / 2.f, 0.5f);
+    const float a = fminf(fnum * (lateral / depth) / 2.f, 0.5f);
     const float c = __cosf(kPi * a);
     return c * c;
 }
@@ -74,234 +122,508 @@ __device__ __forceinline__ float sin_apo(float loc, float centre, float power)
     return r;
 }
 
-__device__ __forceinline__ float2 load_iq(const float2* p) { return __ldg(p); }
-__device__ __forceinline__ float2 load_iq(const __nv_bfloat162* p) { return __bfloat1622float2(__ldg(p)); }
+__device__ __forceinline__ float2 to_f2(float2 v) { return v; }
+__device__ __forceinline__ float2 to_f2(__nv_bfloat162 v) { return __bfloat1622float2(v); }
 
-// Catmull-Rom (tangent 0.5*(p[i+1] - p[i-1])) at fractional position t in [i, i+1],
-// beamformer_utils.cuh:99-125; or linear, :127-140.
-template <bool CUBIC>
-__device__ __forceinline__ float2 interp(float2 pm1, float2 p0, float2 p1, float2 p2, float t)
+// Catmull-Rom (tangent 0.5*(p[i+1] - p[i-1])) at t in [0, 1) between p0 and p1,
+// beamformer_utils.cuh:99-125; linear, :127-140.
+__device__ __forceinline__ float2 catmull_rom(float2 pm1, float2 p0, float2 p1, float2 p2, float t)
 {
-    if constexpr (CUBIC) {
-        const float t2 = t * t;
-        const float h00 = fmaf(fmaf(2.f, t, -3.f), t2, 1.f);
-        const float h10 = fmaf(t - 2.f, t2, t);
-        const float h01 = fmaf(-2.f, t, 3.f) * t2;
-        const float h11 = (t - 1.f) * t2;
-        const float m0x = 0.5f * (p1.x - pm1.x), m0y = 0.5f * (p1.y - pm1.y);
-        const float m1x = 0.5f * (p2.x - p0.x), m1y = 0.5f * (p2.y - p0.y);
-        return make_float2(fmaf(h00, p0.x, fmaf(h01, p1.x, fmaf(h10, m0x, h11 * m1x))),
-                           fmaf(h00, p0.y, fmaf(h01, p1.y, fmaf(h10, m0y, h11 * m1y))));
-    } else {
-        return make_float2(fmaf(p1.x - p0.x, t, p0.x), fmaf(p1.y - p0.y, t, p0.y));
-    }
+    const float t2 = t * t;
+    const float h00 = fmaf(fmaf(2.f, t, -3.f), t2, 1.f);
+    const float h10 = fmaf(t - 2.f, t2, t);
+    const float h01 = fmaf(-2.f, t, 3.f) * t2;
+    const float h11 = (t - 1.f) * t2;
+    const float m0x = 0.5f * (p1.x - pm1.x), m0y = 0.5f * (p1.y - pm1.y);
+    const float m1x = 0.5f * (p2.x - p0.x), m1y = 0.5f * (p2.y - p0.y);
+    return make_float2(fmaf(h00, p0.x, fmaf(h01, p1.x, fmaf(h10, m0x, h11 * m1x))),
+                       fmaf(h00, p0.y, fmaf(h01, p1.y, fmaf(h10, m0y, h11 * m1y))));
 }
 
-// Sample of one row at (already clamped) position idx. `row` is either a staged window
-// (every tap in range) or a global row of n samples whose taps past the end read as 0.
-template <bool CUBIC, bool GUARD, class P>
-__device__ __forceinline__ float2 sample(const P* row, float idx, int n)
+// Guarded read of a global row of n samples; taps past the end read as zero.
+template <bool CUBIC, class IQ>
+__device__ __forceinline__ float2 interp_global(const IQ* row, float idx, int n)
 {
     const int i = __float2int_rd(idx);
     const float t = idx - (float)i;
-    auto tap = [&](int k) -> float2 {
-        if constexpr (GUARD) return k < n ? load_iq(row + k) : make_float2(0.f, 0.f);
-        else return row[k];
-    };
-    if constexpr (CUBIC) return interp<true>(tap(i - 1), tap(i), tap(i + 1), tap(i + 2), t);
-    else return interp<false>(float2{}, tap(i), tap(i + 1), float2{}, t);
+    auto tap = [&](int k) -> float2 { return k < n ? to_f2(__ldg(row + k)) : make_float2(0.f, 0.f); };
+    if constexpr (CUBIC) return catmull_rom(tap(i - 1), tap(i), tap(i + 1), tap(i + 2), t);
+    const float2 p0 = tap(i), p1 = tap(i + 1);
+    return make_float2(fmaf(p1.x - p0.x, t, p0.x), fmaf(p1.y - p0.y, t, p0.y));
 }
 
-template <int SEQ, bool CUBIC, bool CF, class IQ>
-__global__ void __launch_bounds__(kDasThreads)
+// Per-row stage metadata written by the issuing lane.
+struct RowMeta {
+    float base;     // sample index at the tile centre, relative to `lo`
+    float d0;       // FP32 copy of the centre-to-receive-point distance
+    float d0sq;     // its square
+    float two_d0;   // 2 * d0
+    float ex2;      // -2 * (receive point x - centre x)
+    float rx_apo;   // sine receive apodization when it is uniform over the row, else 1
+    float loclamp;  // clamp range of the window-relative index: the row's [1, S-2] ...
+    float hiclamp;  // ... intersected with the staged window
+    int lo;         // row sample of window index 0
+    int len;        // staged samples; 0: the row is read from global memory
+};
+
+// Per-stage metadata (transmit t, sub-signal g, rows c0..c0+nq-1).
+struct StageMeta {
+    float ey2;      // HERCULES: -2 * (receive row y - centre y); FORCES: -2 * (tx element x - centre x)
+    float tx_d0;    // FORCES: centre-to-transmit-element distance
+    float tx_d0sq;
+    float two_tx_d0;
+    float sign;     // READI sign of this sub-signal
+    float uni_apo;  // apodization factor uniform over the stage (sine types)
+    float yj, et;   // receive row y (HERCULES) / transmit element x (FORCES)
+    int t, g, c0, nq;
+};
+
+// Shared memory: NS raw windows per row (TMA destination) and one buffer of cubic
+// coefficients per row: A[i] = (a, b), B[i] = (c, d) with value(t) = a + t (b + t (c + t d))
+// on [i, i + 1] (complex a..d), split so each is one 16-byte load.
+template <class IQ, bool CUBIC>
+struct alignas(128) Smem {
+    IQ raw[kStages][kRows][kWinMax];
+    float4 coefA[CUBIC ? kRows : 1][CUBIC ? kWinMax : 1];
+    float4 coefB[CUBIC ? kRows : 1][CUBIC ? kWinMax : 1];
+    RowMeta rowc[CUBIC ? kRows : 1];  // metadata of the rows whose coefficients are built
+    RowMeta row[kStages][kRows];
+    StageMeta stage[kStages];
+    RowMeta next_row[kBatch][kRows];    // precomputed metadata of the next kBatch stages
+    StageMeta next_stage[kBatch];
+    int next_bytes[kBatch][kRows];
+    uint64_t full[kStages];
+    int abort;
+    int tx_reach_bits;
+};
+
+struct Tile {
+    double cx, cy, cz;  // tile centre (FP64)
+    float radius;       // bound on |voxel - centre| over the tile
+    float tx_reach;     // bound on |transmit-path offset| over the tile, in samples
+};
+
+// Stage k = (transmit t, row chunk, sub-signal g), with g fastest.
+struct StageId {
+    int t, g, c0, nq;
+};
+__device__ __forceinline__ StageId stage_id(const DasArgs& a, int k, int nchunks)
+{
+    StageId s;
+    s.g = k % a.G;
+    const int chunk = (k / a.G) % nchunks;
+    s.t = k / (a.G * nchunks);
+    s.c0 = chunk * kRows;
+    s.nq = min(kRows, a.C - s.c0);
+    return s;
+}
+
+// Stage-uniform geometry, computed by every thread from the stage index.
+template <int SEQ>
+__device__ __forceinline__ StageMeta stage_meta(const DasArgs& a, const StageId& id, const Tile& tile)
+{
+    constexpr bool HERC = SEQ == HERCULES;
+    StageMeta s{};
+    s.t = id.t;
+    s.g = id.g;
+    s.c0 = id.c0;
+    s.nq = id.nq;
+    bool negate = false;
+    if (a.G > 1) {
+        int bit = id.g;
+        if (HERC && a.encoding == WALSH && (id.t & 1)) bit = a.G - 1 - id.g;
+        negate = (a.readi_row >> bit) & 1ull;
+    }
+    s.sign = negate ? -1.f : 1.f;
+    s.uni_apo = 1.f;
+    if (HERC) {
+        const double j = a.G > 1 ? (a.encoding == WALSH ? (double)(id.t * a.G + id.g) : (double)(id.g * a.T + id.t))
+                                 : (double)id.t;
+        const double yj = (double)a.xmin_y + j * (double)a.py;
+        s.yj = (float)yj;
+        s.ey2 = (float)(-2.0 * (yj - tile.cy));
+        if (a.use_apo && a.apo_type == RX_TO_SIN) s.uni_apo = sin_apo(s.yj, a.xmax_y, a.to_power);
+    } else {
+        const double et = (double)a.xmin_x + (double)(id.g * a.T + id.t) * (double)a.px;
+        const double txd0 = sqrt((tile.cx - et) * (tile.cx - et) + tile.cz * tile.cz);
+        s.et = (float)et;
+        s.tx_d0 = (float)txd0;
+        s.tx_d0sq = (float)(txd0 * txd0);
+        s.two_tx_d0 = (float)(2.0 * txd0);
+        s.ey2 = (float)(-2.0 * (et - tile.cx));
+        if (a.use_apo && (a.apo_type == TX_TO_SIN || a.apo_type == BOTH_TO_SIN))
+            s.uni_apo = sin_apo(s.et, a.xmax_x, a.to_power);
+    }
+    return s;
+}
+
+// Window bounds and metadata of row q of stage `id` into batch slot `slot` (one thread per
+// row; all threads of the CTA share the work of a batch of stages).
+template <int SEQ, class IQ, bool CUBIC>
+__device__ void compute_row(Smem<IQ, CUBIC>& sm, int slot, const StageId& id, int q, const DasArgs& a,
+                            const Tile& tile)
+{
+    constexpr bool HERC = SEQ == HERCULES;
+    constexpr int SA = 16 / sizeof(IQ);  // samples per 16-byte unit
+    if (q == 0) sm.next_stage[slot] = stage_meta<SEQ>(a, id, tile);
+    int bytes = 0;
+    RowMeta m{};
+    if (q < id.nq) {
+        const int c = id.c0 + q;
+        const double xc = (double)a.xmin_x + (double)c * (double)a.px;
+        double d0, base;
+        if (HERC) {
+            const double j = a.G > 1 ? (a.encoding == WALSH ? (double)(id.t * a.G + id.g) : (double)(id.g * a.T + id.t))
+                                     : (double)id.t;
+            const double yj = (double)a.xmin_y + j * (double)a.py;
+            const double ex = xc - tile.cx, ey = yj - tile.cy, ez = -tile.cz;
+            d0 = sqrt(ex * ex + ey * ey + ez * ez);
+            // idx = (tx + d + fz) * spm + delay; tx(voxel) = tx(centre) + per-voxel offset.
+            double txc = tile.cz;
+            if (a.focus == 4) {
+                const double dz = tile.cz - (double)a.fz;
+                txc = copysign(sqrt(tile.cy * tile.cy + dz * dz), dz) + (double)a.fz;
+            }
+            base = (txc + d0 + (double)a.fz) * (double)a.spm + (double)a.delay;
+            m.ex2 = (float)(-2.0 * ex);
+        } else {
+            const double et = (double)a.xmin_x + (double)(id.g * a.T + id.t) * (double)a.px;
+            const double txd0 = sqrt((tile.cx - et) * (tile.cx - et) + tile.cz * tile.cz);
+            const double ex = xc - tile.cx;
+            d0 = sqrt(ex * ex + tile.cz * tile.cz);
+            base = (txd0 + d0) * (double)a.spm + (double)a.delay;
+            m.ex2 = (float)(-2.0 * ex);
+        }
+        // Every voxel lies within `radius` of the centre and a path length is 1-Lipschitz, so
+        // the receive part moves the index by at most radius * spm and the transmit part by at
+        // most tile.tx_reach samples.
+        const double reach = (double)tile.radius * (double)a.spm + (double)tile.tx_reach + 1.0;
+        const double smax = (double)a.S - 2.0;
+        const int i_lo = (int)floor(fmin(fmax(base - reach, 1.0), smax));
+        const int i_hi = (int)floor(fmin(fmax(base + reach, 1.0), smax));
+        int lo = max(0, i_lo - 2);
+        const int hi = min(a.S, i_hi + 3);          // sample S is a zero tap
+        lo -= lo % SA;                               // 16-byte aligned start
+        const int len = hi - lo + 1;
+        m.d0 = (float)d0;
+        m.d0sq = (float)(d0 * d0);
+        m.two_d0 = (float)(2.0 * d0);
+        m.rx_apo = 1.f;
+        if (a.use_apo && (a.apo_type == RX_TO_SIN || (!HERC && a.apo_type == BOTH_TO_SIN)))
+            m.rx_apo = sin_apo((float)xc, a.xmax_x, a.to_power);
+        m.lo = lo;
+        m.base = (float)(base - (double)lo);
+        m.loclamp = (float)(1 - lo);
+        m.hiclamp = (float)(a.S - 2 - lo);
+        m.len = 0;
+        if (len + SA <= kWinMax) {
+            m.len = len;
+            m.loclamp = fmaxf(m.loclamp, 1.f);
+            m.hiclamp = fminf(m.hiclamp, (float)(len - 3));
+            const int end = min(hi, a.S - 1);       // last real sample copied
+            int count = end - lo + 1;
+            count += (SA - count % SA) % SA;        // whole 16-byte units; stays inside the row
+            bytes = count * (int)sizeof(IQ);
+        }
+    }
+    sm.next_row[slot][q] = m;
+    sm.next_bytes[slot][q] = bytes;
+}
+
+// Metadata of stages first .. first+kBatch-1 (all threads; a barrier must follow).
+template <int SEQ, class IQ, bool CUBIC>
+__device__ __forceinline__ void compute_batch(Smem<IQ, CUBIC>& sm, int first, int nstages, int nchunks,
+                                              const DasArgs& a, const Tile& tile)
+{
+    for (int i = threadIdx.x; i < kBatch * kRows; i += kThreads) {
+        const int k = first + i / kRows;
+        if (k < nstages) compute_row<SEQ>(sm, (k % kBatch), stage_id(a, k, nchunks), i % kRows, a, tile);
+    }
+}
+
+// Issue stage k into buffer b from its precomputed metadata: lane q of one warp per row.
+template <class IQ, bool CUBIC>
+__device__ __forceinline__ void issue_row(Smem<IQ, CUBIC>& sm, int b, int k, int q, const DasArgs& a,
+                                          const IQ* __restrict__ iq)
+{
+    const int slot = k % kBatch;
+    const StageMeta& st = sm.next_stage[slot];
+    const RowMeta m = sm.next_row[slot][q];
+    const unsigned bytes = (unsigned)sm.next_bytes[slot][q];
+    if (q == 0) sm.stage[b] = st;
+    sm.row[b][q] = m;
+    if (bytes && m.lo + m.len - 1 == a.S) sm.raw[b][q][a.S - m.lo] = IQ{};  // zero tap past the row end
+    // Order earlier generic-proxy accesses of this buffer before the async-proxy writes.
+    fence_proxy_async();
+    mbar_arrive_expect_tx(&sm.full[b], bytes);
+    if (bytes) bulk_load(&sm.raw[b][q][0], iq + ((size_t)st.t * a.C + st.c0 + q) * a.S + m.lo, bytes, &sm.full[b]);
+}
+
+// Distance correction d - d0 from d^2 - d0^2 = delta: one approximate reciprocal square root
+// and a Newton step on (d0 + e)^2 = d0^2 + delta, exact to FP32 rounding of the small terms.
+__device__ __forceinline__ float path_offset(float delta, float d0, float d0sq, float two_d0)
+{
+    const float D = d0sq + delta;
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(D));
+    const float e0 = fmaf(D, r, -d0);
+    const float res = fmaf(e0, e0 + two_d0, -delta);
+    return fmaf(-0.5f * r, res, e0);
+}
+
+// Cubic coefficients of every staged interval of stage buffer b (all threads).
+template <class IQ>
+__device__ __forceinline__ void build_coefficients(Smem<IQ, true>& sm, int b, int nq)
+{
+    if (threadIdx.x < nq) sm.rowc[threadIdx.x] = sm.row[b][threadIdx.x];
+    for (int q = 0; q < nq; ++q) {
+        const int len = sm.row[b][q].len;
+        const IQ* p = &sm.raw[b][q][0];
+        for (int i = 1 + threadIdx.x; i <= len - 3; i += kThreads) {
+            const float2 pm1 = to_f2(p[i - 1]), p0 = to_f2(p[i]), p1 = to_f2(p[i + 1]), p2 = to_f2(p[i + 2]);
+            float4 A, B;
+            A.x = p0.x;
+            A.y = p0.y;
+            A.z = 0.5f * (p1.x - pm1.x);
+            A.w = 0.5f * (p1.y - pm1.y);
+            B.x = fmaf(-0.5f, p2.x, fmaf(2.f, p1.x, fmaf(-2.5f, p0.x, pm1.x)));
+            B.y = fmaf(-0.5f, p2.y, fmaf(2.f, p1.y, fmaf(-2.5f, p0.y, pm1.y)));
+            B.z = fmaf(0.5f, p2.x - pm1.x, 1.5f * (p0.x - p1.x));
+            B.w = fmaf(0.5f, p2.y - pm1.y, 1.5f * (p0.y - p1.y));
+            sm.coefA[q][i] = A;
+            sm.coefB[q][i] = B;
+        }
+    }
+}
+
+// Accumulates one row into the thread's voxels. STAGED: from shared memory (coefficients
+// for cubic, raw taps for linear); otherwise from the global row with guarded taps.
+template <int SEQ, bool CUBIC, bool CF, bool APO, bool STAGED, class IQ, bool CUBIC_SM>
+__device__ __forceinline__ void row_pass(const DasArgs& a, const Smem<IQ, CUBIC_SM>& sm, const RowMeta* rows, int b,
+                                         int qi, const IQ* grow, const StageMeta& st, float dxe, const float (&sq)[kVpt],
+                                         const float (&txs)[kVpt], const float (&vzv)[kVpt], float vx, float a2,
+                                         float2 (&total)[kVpt], float (&inc)[kVpt])
+{
+    constexpr bool HERC = SEQ == HERCULES;
+    constexpr float kMagic = 8388608.f;  // 2^23: adding it with round-down leaves floor(x) in the mantissa
+    const RowMeta& m = rows[qi];
+    const float exdx = m.ex2 * dxe;
+    const float base = m.base, d0 = m.d0, d0sq = m.d0sq, two_d0 = m.two_d0;
+    const float loc = m.loclamp, hic = m.hiclamp;
+    float xc = 0.f;
+    if (APO) xc = (float)((double)a.xmin_x + (double)(st.c0 + qi) * (double)a.px);
+#pragma unroll
+    for (int v = 0; v < kVpt; ++v) {
+        const float corr = path_offset(exdx + sq[v], d0, d0sq, two_d0);
+        float w = st.sign;
+        if (APO) {
+            float apo;
+            const float rx = xc - vx;
+            if (HERC) {
+                apo = a.apo_type == RX_TO_SIN ? m.rx_apo * st.uni_apo
+                                              : hann_apo(sqrtf(fmaf(rx, rx, a2)), vzv[v], a.fn_rx);
+                if (!(apo > 0.1f)) continue;
+            } else {
+                const float ra = (a.apo_type == RX_TO_SIN || a.apo_type == BOTH_TO_SIN)
+                                     ? m.rx_apo
+                                     : hann_apo(fabsf(rx), vzv[v], a.fn_rx);
+                if (!(ra > 0.f)) continue;
+                const float ta = (a.apo_type == TX_TO_SIN || a.apo_type == BOTH_TO_SIN)
+                                     ? st.uni_apo
+                                     : hann_apo(fabsf(vx - st.et), vzv[v], a.fn_tx);
+                apo = ra * ta;
+            }
+            w *= apo;
+        }
+        float idx = fmaf(corr, a.spm, base + txs[v]);
+        idx = fminf(fmaxf(idx, loc), hic);
+        float2 val;
+        if (STAGED) {
+            const float f = __fadd_rd(idx, kMagic);
+            const int i = __float_as_int(f) - __float_as_int(kMagic);
+            const float t = idx - (f - kMagic);
+            if constexpr (CUBIC) {
+                const float4 A = sm.coefA[qi][i], B = sm.coefB[qi][i];
+                val.x = fmaf(fmaf(fmaf(B.z, t, B.x), t, A.z), t, A.x);
+                val.y = fmaf(fmaf(fmaf(B.w, t, B.y), t, A.w), t, A.y);
+            } else {
+                const IQ* p = &sm.raw[b][qi][i];
+                const float2 p0 = to_f2(p[0]), p1 = to_f2(p[1]);
+                val = make_float2(fmaf(p1.x - p0.x, t, p0.x), fmaf(p1.y - p0.y, t, p0.y));
+            }
+        } else {
+            val = interp_global<CUBIC>(grow + m.lo, idx, a.S - m.lo);
+        }
+        total[v].x = fmaf(w, val.x, total[v].x);
+        total[v].y = fmaf(w, val.y, total[v].y);
+        if (CF) inc[v] = fmaf(val.x, val.x, fmaf(val.y, val.y, inc[v]));
+    }
+}
+
+// Thread layout. HERCULES: lanes are 4 (x) x 8 (y) neighbours, whose delays differ by less
+// than a sample or two, so their shared-memory reads fall in distinct banks or broadcast;
+// warps and the kVpt registers of a thread run along z. FORCES (no y): lanes along x.
+template <int SEQ>
+struct Layout {
+    static constexpr int TX = SEQ == HERCULES ? 4 : 32;
+    static constexpr int TY = SEQ == HERCULES ? 8 : 1;
+    static constexpr int TZ = kWarps * kVpt;
+};
+
+template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ>
+__global__ void __launch_bounds__(kThreads, 3)
 das_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
 {
-    __shared__ float2 win[kCps][kWinStride];
-    __shared__ int s_lo[kCps], s_len[kCps];
-
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    auto& sm = *reinterpret_cast<Smem<IQ, CUBIC>*>(smem_raw);
     constexpr bool HERC = SEQ == HERCULES;
+    using L = Layout<SEQ>;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-    // ---- voxels of this thread and the tile box -------------------------------------
-    const int x_base = HERC ? blockIdx.x * kVpt : blockIdx.x * (8 * kVpt) + warp * kVpt;
-    const int y_idx = HERC ? blockIdx.y * 8 + warp : 0;
-    const int z_idx = blockIdx.z * 32 + lane;
-    const bool yz_ok = y_idx < a.Y && z_idx < a.Z;
-    const float vy = fmaf((float)min(y_idx, a.Y - 1), a.res_y, a.vmin_y);
-    const float vz = fmaf((float)min(z_idx, a.Z - 1), a.res_z, a.vmin_z);
-    float vx[kVpt];
-#pragma unroll
-    for (int v = 0; v < kVpt; ++v) vx[v] = fmaf((float)min(x_base + v, a.X - 1), a.res_x, a.vmin_x);
-
-    // Tile bounding box over the voxels that exist (uniform across the CTA).
-    const int tx0 = HERC ? blockIdx.x * kVpt : blockIdx.x * 8 * kVpt;
-    const int tx1 = min(tx0 + (HERC ? kVpt : 8 * kVpt), a.X) - 1;
-    const int ty0 = HERC ? blockIdx.y * 8 : 0, ty1 = HERC ? min(ty0 + 8, a.Y) - 1 : 0;
-    const int tz0 = blockIdx.z * 32, tz1 = min(tz0 + 32, a.Z) - 1;
-    const float bx0 = fminf(fmaf((float)tx0, a.res_x, a.vmin_x), fmaf((float)tx1, a.res_x, a.vmin_x));
-    const float bx1 = fmaxf(fmaf((float)tx0, a.res_x, a.vmin_x), fmaf((float)tx1, a.res_x, a.vmin_x));
-    const float by0 = fminf(fmaf((float)ty0, a.res_y, a.vmin_y), fmaf((float)ty1, a.res_y, a.vmin_y));
-    const float by1 = fmaxf(fmaf((float)ty0, a.res_y, a.vmin_y), fmaf((float)ty1, a.res_y, a.vmin_y));
-    const float bz0 = fminf(fmaf((float)tz0, a.res_z, a.vmin_z), fmaf((float)tz1, a.res_z, a.vmin_z));
-    const float bz1 = fmaxf(fmaf((float)tz0, a.res_z, a.vmin_z), fmaf((float)tz1, a.res_z, a.vmin_z));
-    const Interval vz2 = sq_range(bz0, bz1);
-
-    // Transmit distance (HERCULES; templated_beamformer.cuh:16-40, :136-147) and its range.
-    float txd = vz;
-    Interval txr = {bz0, bz1};
-    if (HERC && a.focus == 4) {  // YZ_FOCUS
-        const float dz = vz - a.fz;
-        txd = copysignf(sqrtf(vy * vy + dz * dz), dz) + a.fz;
-        const Interval vy2 = sq_range(by0, by1);
-        const float dz0 = bz0 - a.fz, dz1 = bz1 - a.fz;
-        const Interval dz2 = sq_range(dz0, dz1);
-        const float rlo = sqrtf(vy2.lo + dz2.lo), rhi = sqrtf(vy2.hi + dz2.hi);
-        txr.lo = (dz0 >= 0.f ? rlo : -rhi) + a.fz;
-        txr.hi = (dz1 <= 0.f ? -rlo : rhi) + a.fz;
+    // ---- tile, voxels, offsets from the tile centre -----------------------------------------
+    const int tx0 = blockIdx.x * L::TX, ty0 = blockIdx.y * L::TY, tz0 = blockIdx.z * L::TZ;
+    const float ix_c = tx0 + 0.5f * (L::TX - 1), iy_c = ty0 + 0.5f * (L::TY - 1), iz_c = tz0 + 0.5f * (L::TZ - 1);
+    Tile tile;
+    tile.cx = (double)a.vmin_x + (double)ix_c * (double)a.res_x;
+    tile.cy = HERC ? (double)a.vmin_y + (double)iy_c * (double)a.res_y : 0.0;
+    tile.cz = (double)a.vmin_z + (double)iz_c * (double)a.res_z;
+    {
+        const double hx = 0.5 * (L::TX - 1) * fabs((double)a.res_x);
+        const double hy = HERC ? 0.5 * (L::TY - 1) * fabs((double)a.res_y) : 0.0;
+        const double hz = 0.5 * (L::TZ - 1) * fabs((double)a.res_z);
+        tile.radius = (float)(sqrt(hx * hx + hy * hy + hz * hz) * (1.0 + 1e-6) + 1e-9);
     }
+    const int x_idx = tx0 + (HERC ? (lane & 3) : lane);
+    const int y_idx = HERC ? ty0 + (lane >> 2) : 0;
+    const int z_first = tz0 + warp * kVpt;
+    // Offsets in voxel units are exact in FP32; scaled by the step they carry one rounding.
+    const float dxe = ((float)x_idx - ix_c) * a.res_x;
+    const float dye = HERC ? ((float)y_idx - iy_c) * a.res_y : 0.f;
+    const float vx = fmaf((float)x_idx, a.res_x, a.vmin_x);
+    const float vy = fmaf((float)y_idx, a.res_y, a.vmin_y);
+    float dz[kVpt], vzv[kVpt], txs[kVpt];
+#pragma unroll
+    for (int v = 0; v < kVpt; ++v) {
+        dz[v] = ((float)(z_first + v) - iz_c) * a.res_z;
+        vzv[v] = fmaf((float)(z_first + v), a.res_z, a.vmin_z);
+        txs[v] = 0.f;
+        if (HERC) {
+            // Transmit path of this voxel relative to the centre's (FP64), in samples.
+            double tx_rel = (double)dz[v];
+            if (a.focus == 4) {
+                const double vyd = tile.cy + (double)dye, dzf = tile.cz + (double)dz[v] - (double)a.fz;
+                const double dzc = tile.cz - (double)a.fz;
+                tx_rel = copysign(sqrt(vyd * vyd + dzf * dzf), dzf) - copysign(sqrt(tile.cy * tile.cy + dzc * dzc), dzc);
+            }
+            txs[v] = (float)(tx_rel * (double)a.spm);
+        }
+    }
+    // Largest transmit offset over the tile (a focused transmit path jumps across the focal
+    // depth, so it is measured rather than bounded). FORCES: the transmit path is 1-Lipschitz.
+    if (threadIdx.x == 0) {
+        sm.tx_reach_bits = 0;
+        sm.abort = 0;
+        for (int b = 0; b < kStages; ++b) mbar_init(&sm.full[b], kRows);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (HERC) {
+        float mx = 0.f;
+#pragma unroll
+        for (int v = 0; v < kVpt; ++v) mx = fmaxf(mx, fabsf(txs[v]));
+        atomicMax(&sm.tx_reach_bits, __float_as_int(mx * 1.0001f + 1e-3f));
+    }
+    __syncthreads();
+    tile.tx_reach = HERC ? __int_as_float(sm.tx_reach_bits) : tile.radius * a.spm;
+
+    // |delta|^2 and the z part of -2 (e - centre).delta, per voxel.
+    const float two_cz = (float)(2.0 * tile.cz);
+    float qz[kVpt];
+#pragma unroll
+    for (int v = 0; v < kVpt; ++v) qz[v] = fmaf(two_cz, dz[v], fmaf(dxe, dxe, fmaf(dye, dye, dz[v] * dz[v])));
 
     float2 total[kVpt];
     float inc[kVpt];
 #pragma unroll
-    for (int v = 0; v < kVpt; ++v) { total[v] = make_float2(0.f, 0.f); inc[v] = 0.f; }
-
-    const float spm = a.spm;
-    const float smax = (float)a.S - 2.f;
-
-    for (int t = 0; t < a.T; ++t) {
-        for (int c0 = 0; c0 < a.C; c0 += kCps) {
-            const int nq = min(kCps, a.C - c0);
-            // ---- window of samples the tile can address in each staged row -------------
-            if (threadIdx.x < nq) {
-                const int c = c0 + threadIdx.x;
-                float imin = INFINITY, imax = -INFINITY;
-                if (HERC) {
-                    const float xc = fmaf((float)c, a.px, a.xmin_x);
-                    const Interval rx2 = sq_range(xc - bx1, xc - bx0);
-                    for (int g = 0; g < a.G; ++g) {
-                        const float j = a.G > 1 ? (a.encoding == WALSH ? (float)(t * a.G + g) : (float)(g * a.T + t))
-                                                : (float)t;
-                        const float yj = fmaf(j, a.py, a.xmin_y);
-                        const Interval ry2 = sq_range(yj - by1, yj - by0);
-                        imin = fminf(imin, (txr.lo + sqrtf(rx2.lo + ry2.lo + vz2.lo) + a.fz) * spm + a.delay);
-                        imax = fmaxf(imax, (txr.hi + sqrtf(rx2.hi + ry2.hi + vz2.hi) + a.fz) * spm + a.delay);
-                    }
-                } else {
-                    const float ec = fmaf((float)c, a.px, a.xmin_x);
-                    const Interval rx2 = sq_range(ec - bx1, ec - bx0);
-                    const float rlo = sqrtf(rx2.lo + vz2.lo), rhi = sqrtf(rx2.hi + vz2.hi);
-                    for (int g = 0; g < a.G; ++g) {
-                        const float et = fmaf((float)(g * a.T + t), a.px, a.xmin_x);
-                        const Interval tx2 = sq_range(bx0 - et, bx1 - et);
-                        imin = fminf(imin, (sqrtf(tx2.lo + vz2.lo) + rlo) * spm + a.delay);
-                        imax = fmaxf(imax, (sqrtf(tx2.hi + vz2.hi) + rhi) * spm + a.delay);
-                    }
-                }
-                int lo = 0, len = 0;
-                if (imin <= imax) {  // false for NaN bounds: use the guarded direct path
-                    imin = fminf(fmaxf(imin, 1.f), smax);
-                    imax = fminf(fmaxf(imax, 1.f), smax);
-                    lo = max(0, (int)floorf(imin) - 3);
-                    const int hi = min(a.S, (int)floorf(imax) + 4);  // index S is a zero tap
-                    len = hi - lo + 1;
-                    if (len > kWinMax) { lo = 0; len = 0; }
-                }
-                s_lo[threadIdx.x] = lo;
-                s_len[threadIdx.x] = len;
-            }
-            __syncthreads();
-            // ---- stage the windows ------------------------------------------------------
-            for (int q = 0; q < nq; ++q) {
-                const int len = s_len[q], lo = s_lo[q];
-                const IQ* row = iq + ((size_t)t * a.C + c0 + q) * a.S;
-                for (int i = threadIdx.x; i < len; i += kDasThreads)
-                    win[q][i] = lo + i < a.S ? load_iq(row + lo + i) : make_float2(0.f, 0.f);
-            }
-            __syncthreads();
-            // ---- accumulate ---------------------------------------------------------------
-            for (int g = 0; g < a.G; ++g) {
-                bool negate = false;
-                float ry = 0.f, a2 = 0.f, et = 0.f, yj = 0.f;
-                if (a.G > 1) {
-                    int bit = g;
-                    if (HERC && a.encoding == WALSH && (t & 1)) bit = a.G - 1 - g;
-                    negate = (a.readi_row >> bit) & 1ull;
-                }
-                if (HERC) {
-                    const float j = a.G > 1 ? (a.encoding == WALSH ? (float)(t * a.G + g) : (float)(g * a.T + t))
-                                            : (float)t;
-                    yj = fmaf(j, a.py, a.xmin_y);
-                    ry = yj - vy;
-                    a2 = fmaf(ry, ry, vz * vz);
-                } else {
-                    et = fmaf((float)(g * a.T + t), a.px, a.xmin_x);
-                }
-                for (int q = 0; q < nq; ++q) {
-                    const int c = c0 + q;
-                    const int len = s_len[q];
-                    const bool staged = len > 0;
-                    const float lo = (float)s_lo[q];
-                    const float hiclamp = staged ? (float)(len - 3) : smax;
-                    const float xc = fmaf((float)c, a.px, a.xmin_x);
-                    const IQ* grow = iq + ((size_t)t * a.C + c) * a.S;
-                    float rx_apo = 1.f, uni_apo = 1.f;
-                    if (a.use_apo) {
-                        if (HERC) {
-                            if (a.apo_type == RX_TO_SIN)
-                                uni_apo = sin_apo(xc, a.xmax_x, a.to_power) * sin_apo(yj, a.xmax_y, a.to_power);
-                        } else {
-                            if (a.apo_type == RX_TO_SIN || a.apo_type == BOTH_TO_SIN)
-                                rx_apo = sin_apo(xc, a.xmax_x, a.to_power);
-                            if (a.apo_type == TX_TO_SIN || a.apo_type == BOTH_TO_SIN)
-                                uni_apo = sin_apo(et, a.xmax_x, a.to_power);
-                        }
-                    }
-#pragma unroll
-                    for (int v = 0; v < kVpt; ++v) {
-                        const float rx = xc - vx[v];
-                        float d, apo = 1.f;
-                        if (HERC) {
-                            d = txd + fast_sqrt(fmaf(rx, rx, a2));
-                            if (a.use_apo) {
-                                apo = a.apo_type == RX_TO_SIN ? uni_apo
-                                                              : hann_apo(sqrtf(fmaf(rx, rx, ry * ry)), vz, a.fn_rx);
-                                if (!(apo > 0.1f)) continue;
-                            }
-                            d += a.fz;
-                        } else {
-                            const float txx = vx[v] - et;
-                            d = fast_sqrt(fmaf(txx, txx, vz * vz)) + fast_sqrt(fmaf(rx, rx, vz * vz));
-                            if (a.use_apo) {
-                                float ra = rx_apo;
-                                if (!(a.apo_type == RX_TO_SIN || a.apo_type == BOTH_TO_SIN))
-                                    ra = hann_apo(fabsf(rx), vz, a.fn_rx);
-                                if (!(ra > 0.f)) continue;
-                                const float ta = (a.apo_type == TX_TO_SIN || a.apo_type == BOTH_TO_SIN)
-                                                     ? uni_apo
-                                                     : hann_apo(fabsf(txx), vz, a.fn_tx);
-                                apo = ra * ta;
-                            }
-                        }
-                        float idx = fmaf(d, spm, a.delay) - lo;
-                        idx = fminf(fmaxf(idx, 1.f), hiclamp);
-                        const float2 val = staged ? sample<CUBIC, false>(win[q], idx, 0)
-                                                  : sample<CUBIC, true>(grow, idx, a.S);
-                        const float w = negate ? -apo : apo;
-                        total[v].x = fmaf(w, val.x, total[v].x);
-                        total[v].y = fmaf(w, val.y, total[v].y);
-                        inc[v] = fmaf(val.x, val.x, fmaf(val.y, val.y, inc[v]));
-                    }
-                }
-            }
-            __syncthreads();
-        }
+    for (int v = 0; v < kVpt; ++v) {
+        total[v] = make_float2(0.f, 0.f);
+        inc[v] = 0.f;
     }
 
-    if (!yz_ok) return;
+    const int nchunks = div_up(a.C, kRows);
+    const int nstages = a.T * nchunks * a.G;
+    // Window metadata (FP64) is computed for kBatch stages at a time by all threads; a stage's
+    // bulk copies are then issued by lanes 0..kRows-1 of warp 0, one row per lane.
+    static_assert(kRows <= 32 && kStages <= kBatch, "issue layout");
+    compute_batch<SEQ>(sm, 0, nstages, nchunks, a, tile);
+    __syncthreads();
+    if (warp == 0 && lane < kRows)
+        for (int k = 0; k < kStages && k < nstages; ++k) issue_row(sm, k, k, lane, a, iq);
+
+    for (int k = 0; k < nstages; ++k) {
+        const int b = k % kStages;
+        if (!mbar_wait_bounded(&sm.full[b], (unsigned)(k / kStages) & 1u)) {
+            sm.abort = 1;
+            atomicOr(a.status, 1);
+        }
+        const StageMeta st = sm.stage[b];
+        const int next = k + kStages;  // stage that refills buffer b
+        if (next < nstages && next % kBatch == 0) compute_batch<SEQ>(sm, next, nstages, nchunks, a, tile);
+        int all_staged = 1;
+        if constexpr (CUBIC) {
+            build_coefficients(sm, b, st.nq);
+            all_staged = __syncthreads_and(threadIdx.x >= st.nq || sm.row[b][threadIdx.x].len > 0);
+            // The raw buffer is free once transformed: refill it while this stage computes.
+            if (warp == 0 && lane < kRows && next < nstages && !sm.abort) issue_row(sm, b, next, lane, a, iq);
+        }
+        const RowMeta* rows = CUBIC ? sm.rowc : sm.row[b];
+        if (!CUBIC)
+            for (int q = 0; q < st.nq; ++q) all_staged &= rows[q].len > 0;
+        // Per-stage, per-voxel part of d^2 - d0^2 (receive path) and the FORCES transmit offset.
+        float sq[kVpt], tsh[kVpt];
+        float a2 = 0.f;
+        if (APO && HERC) a2 = (st.yj - vy) * (st.yj - vy);
+#pragma unroll
+        for (int v = 0; v < kVpt; ++v) {
+            if (HERC) {
+                sq[v] = fmaf(st.ey2, dye, qz[v]);
+                tsh[v] = txs[v];
+            } else {
+                sq[v] = qz[v];
+                tsh[v] = path_offset(fmaf(st.ey2, dxe, qz[v]), st.tx_d0, st.tx_d0sq, st.two_tx_d0) * a.spm;
+            }
+        }
+        const IQ* grow0 = iq + ((size_t)st.t * a.C + st.c0) * a.S;
+        if (all_staged) {
+#pragma unroll 2
+            for (int qi = 0; qi < st.nq; ++qi)
+                row_pass<SEQ, CUBIC, CF, APO, true>(a, sm, rows, b, qi, grow0, st, dxe, sq, tsh, vzv, vx, a2, total,
+                                                    inc);
+        } else {
+            for (int qi = 0; qi < st.nq; ++qi) {
+                if (rows[qi].len > 0)
+                    row_pass<SEQ, CUBIC, CF, APO, true>(a, sm, rows, b, qi, grow0, st, dxe, sq, tsh, vzv, vx, a2, total,
+                                                        inc);
+                else
+                    row_pass<SEQ, CUBIC, CF, APO, false>(a, sm, rows, b, qi, grow0 + (size_t)qi * a.S, st, dxe, sq, tsh,
+                                                         vzv, vx, a2, total, inc);
+            }
+        }
+        __syncthreads();
+        if (sm.abort) break;
+        if (!CUBIC && warp == 0 && lane < kRows && next < nstages) issue_row(sm, b, next, lane, a, iq);
+    }
+    if (sm.abort) {
+        // Let every copy already issued land before the CTA's shared memory is released.
+        for (int k = 0; k < kStages; ++k) mbar_wait_bounded(&sm.full[k], 0), mbar_wait_bounded(&sm.full[k], 1);
+        return;
+    }
+
+    if (x_idx >= a.X || y_idx >= a.Y) return;
 #pragma unroll
     for (int v = 0; v < kVpt; ++v) {
-        const int x = x_base + v;
-        if (x >= a.X) continue;
+        const int z = z_first + v;
+        if (z >= a.Z) continue;
         float2 out = total[v];
         if (CF) {
             float cf = powf((out.x * out.x + out.y * out.y) / inc[v], a.cf_power);
@@ -310,21 +632,27 @@ das_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
             out.y *= cf;
         }
         if (HERC) {
-            vol[((size_t)z_idx * a.Y + y_idx) * a.X + x] = out;
+            vol[((size_t)z * a.Y + y_idx) * a.X + x_idx] = out;
         } else {
-            for (int y = 0; y < a.Y; ++y) vol[((size_t)z_idx * a.Y + y) * a.X + x] = out;
+            for (int y = 0; y < a.Y; ++y) vol[((size_t)z * a.Y + y) * a.X + x_idx] = out;
         }
     }
 }
 
-template <int SEQ, bool CUBIC, bool CF, class IQ>
+template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ>
 bool launch_das_t(const DasArgs& a, const void* iq, void* volume, cudaStream_t st)
 {
-    dim3 grid;
-    if (SEQ == HERCULES) grid = dim3(div_up(a.X, kVpt), div_up(a.Y, 8), div_up(a.Z, 32));
-    else grid = dim3(div_up(a.X, 8 * kVpt), 1, div_up(a.Z, 32));
+    using L = Layout<SEQ>;
+    const dim3 grid(div_up(a.X, L::TX), div_up(a.Y, L::TY), div_up(a.Z, L::TZ));
     CUTB_REQUIRE(grid.y <= 65535 && grid.z <= 65535, CUTB_ERR_UNSUPPORTED, "Output grid too large.");
-    das_kernel<SEQ, CUBIC, CF, IQ><<<grid, kDasThreads, 0, st>>>((const IQ*)iq, (float2*)volume, a);
+    auto kern = das_kernel<SEQ, CUBIC, CF, APO, IQ>;
+    const size_t smem = sizeof(Smem<IQ, CUBIC>);
+    static bool configured = false;
+    if (!configured) {
+        CUTB_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = true;
+    }
+    kern<<<grid, kThreads, smem, st>>>((const IQ*)iq, (float2*)volume, a);
     CUTB_CUDA_OK(cudaGetLastError());
     return true;
 }
@@ -332,10 +660,19 @@ bool launch_das_t(const DasArgs& a, const void* iq, void* volume, cudaStream_t s
 template <int SEQ, class IQ>
 bool launch_das_s(const DasArgs& a, const void* iq, void* volume, cudaStream_t st)
 {
-    if (a.cubic) return a.apply_cf ? launch_das_t<SEQ, true, true, IQ>(a, iq, volume, st)
-                                   : launch_das_t<SEQ, true, false, IQ>(a, iq, volume, st);
-    return a.apply_cf ? launch_das_t<SEQ, false, true, IQ>(a, iq, volume, st)
-                      : launch_das_t<SEQ, false, false, IQ>(a, iq, volume, st);
+#define CUTB_DAS_CASE(CUBIC, CF, APO)                                                   \
+    if ((bool)a.cubic == CUBIC && (bool)a.apply_cf == CF && (bool)a.use_apo == APO) \
+        return launch_das_t<SEQ, CUBIC, CF, APO, IQ>(a, iq, volume, st);
+    CUTB_DAS_CASE(true, true, false)
+    CUTB_DAS_CASE(true, false, false)
+    CUTB_DAS_CASE(false, true, false)
+    CUTB_DAS_CASE(false, false, false)
+    CUTB_DAS_CASE(true, true, true)
+    CUTB_DAS_CASE(true, false, true)
+    CUTB_DAS_CASE(false, true, true)
+    CUTB_DAS_CASE(false, false, true)
+#undef CUTB_DAS_CASE
+    return false;
 }
 
 }  // namespace
@@ -381,6 +718,9 @@ bool derive_das(const CudaBeamformerParameters& bp, DasArgs& a)
     a.res_x = a.X > 1 ? (bp.output_max_coordinate[0] - bp.output_min_coordinate[0]) / (float)(a.X - 1) : 0.f;
     a.res_y = a.res_x;
     a.res_z = a.Z > 1 ? (bp.output_max_coordinate[2] - bp.output_min_coordinate[2]) / (float)(a.Z - 1) : 0.f;
+    CUTB_REQUIRE(std::isfinite(a.res_x) && std::isfinite(a.res_z) && std::isfinite(a.vmin_x) &&
+                     std::isfinite(a.vmin_y) && std::isfinite(a.vmin_z),
+                 CUTB_ERR_INVALID_ARGUMENT, "Output grid coordinates must be finite.");
     a.fn_rx = bp.fn_rx;
     a.fn_tx = bp.fn_tx;
     a.cf_power = fminf(fmaxf(bp.coherency_weighting, 0.f), 1.f);
@@ -438,6 +778,11 @@ bool derive_das(const CudaBeamformerParameters& bp, DasArgs& a)
 
 bool launch_das(const DasArgs& a, const void* iq, bool iq_bf16, void* volume, cudaStream_t st, int* launches)
 {
+    CUTB_REQUIRE(a.status != nullptr, CUTB_ERR_NOT_INITIALIZED, "Delay-and-sum status word not allocated.");
+    CUTB_REQUIRE((uintptr_t)iq % 16 == 0, CUTB_ERR_INVALID_ARGUMENT,
+                 "The analytic-signal buffer must be 16-byte aligned.");
+    CUTB_REQUIRE(a.S % 4 == 0, CUTB_ERR_UNSUPPORTED,
+                 "Delay-and-sum needs a sample count that is a multiple of 4 (got %d).", a.S);
     bool ok;
     if (a.seq == HERCULES)
         ok = iq_bf16 ? launch_das_s<HERCULES, __nv_bfloat162>(a, iq, volume, st)

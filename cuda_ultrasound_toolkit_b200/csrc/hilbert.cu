@@ -48,14 +48,25 @@ __device__ __forceinline__ void run_fft(cplx (&x)[16], uint32_t tau, const cplx*
     }
 }
 
-__device__ __forceinline__ void store_iq(float2* out, uint64_t i, float re, float im) { out[i] = make_float2(re, im); }
-__device__ __forceinline__ void store_iq(__nv_bfloat162* out, uint64_t i, float re, float im)
+// Writes one component (PART 0 = real, 1 = imaginary) of output sample i.
+template <int PART>
+__device__ __forceinline__ void store_part(float2* out, uint64_t i, float v)
 {
-    out[i] = __floats2bfloat162_rn(re, im);
+    reinterpret_cast<float*>(out + i)[PART] = v;
+}
+template <int PART>
+__device__ __forceinline__ void store_part(__nv_bfloat162* out, uint64_t i, float v)
+{
+    reinterpret_cast<__nv_bfloat16*>(out + i)[PART] = __float2bfloat16_rn(v);
 }
 
+template <int LOGN>
+constexpr int hilbert_threads() { return hilbert_fft_per_block<LOGN>() * (1 << LOGN) / 16; }
+template <int LOGN>
+constexpr int hilbert_min_blocks() { return hilbert_threads<LOGN>() <= 256 ? 2 : 1; }
+
 template <int LOGN, class OutT>
-__global__ void __launch_bounds__(hilbert_fft_per_block<LOGN>() * (1 << LOGN) / 16)
+__global__ void __launch_bounds__(hilbert_threads<LOGN>(), hilbert_min_blocks<LOGN>())
 hilbert_kernel(const float* __restrict__ in, OutT* __restrict__ out, HilbertArgs a)
 {
     constexpr uint32_t N = 1u << LOGN;
@@ -81,23 +92,32 @@ hilbert_kernel(const float* __restrict__ in, OutT* __restrict__ out, HilbertArgs
     }
     run_fft<LOGN, -1>(z, tau, tw, sre, sim);  // z[m] = Z[tau + m*TPF]
 
-    const cplx* ge = reinterpret_cast<const cplx*>(a.ge);
-    const cplx* go = reinterpret_cast<const cplx*>(a.go);
-    cplx r1[16], w[16];
+    const float2* ge = reinterpret_cast<const float2*>(a.ge);
+    const float2* go = reinterpret_cast<const float2*>(a.go);
+    auto weight = [](const float2* t, uint32_t k) {
+        const float2 v = __ldg(t + k);
+        return cplx{v.x, v.y};
+    };
+    cplx w[16];
+    // IDFT(Z Ge) = Re(iq_a) + i Re(iq_b): written to the real parts.
 #pragma unroll
-    for (int m = 0; m < 16; ++m) r1[m] = fft::cmul(z[m], ge[tau + m * TPF]);
-    __syncthreads();
-    run_fft<LOGN, +1>(r1, tau, tw, sre, sim);
-#pragma unroll
-    for (int m = 0; m < 16; ++m) w[m] = fft::cmul(z[m], go[tau + m * TPF]);
-    __syncthreads();
+    for (int m = 0; m < 16; ++m) w[m] = fft::cmul(z[m], weight(ge, tau + m * TPF));
     run_fft<LOGN, +1>(w, tau, tw, sre, sim);
-
 #pragma unroll
     for (int m = 0; m < 16; ++m) {
         const uint64_t n = tau + m * TPF;
-        if (has_a) store_iq(out, ra * N + n, r1[m].x, w[m].x);
-        if (has_b) store_iq(out, rb * N + n, r1[m].y, w[m].y);
+        if (has_a) store_part<0>(out, ra * N + n, w[m].x);
+        if (has_b) store_part<0>(out, rb * N + n, w[m].y);
+    }
+    // IDFT(Z Go) = Im(iq_a) + i Im(iq_b): written to the imaginary parts.
+#pragma unroll
+    for (int m = 0; m < 16; ++m) w[m] = fft::cmul(z[m], weight(go, tau + m * TPF));
+    run_fft<LOGN, +1>(w, tau, tw, sre, sim);
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const uint64_t n = tau + m * TPF;
+        if (has_a) store_part<1>(out, ra * N + n, w[m].x);
+        if (has_b) store_part<1>(out, rb * N + n, w[m].y);
     }
 }
 
@@ -116,7 +136,7 @@ bool launch_hilbert_t(const float* in, void* out, const HilbertArgs& a, cudaStre
     const uint64_t pairs = (a.rows + 1) / 2;
     const uint64_t blocks = div_up(pairs, (uint64_t)FPB);
     CUTB_REQUIRE(blocks <= 0x7fffffffull, CUTB_ERR_INVALID_ARGUMENT, "Too many rows for one launch.");
-    kern<<<(unsigned)blocks, FPB * (N / 16), smem, st>>>(in, (OutT*)out, a);
+    kern<<<(unsigned)blocks, hilbert_threads<LOGN>(), smem, st>>>(in, (OutT*)out, a);
     CUTB_CUDA_OK(cudaGetLastError());
     return true;
 }

@@ -285,6 +285,20 @@ CUTB_API bool cutb_das(cutb_plan* p, const void* d_iq, void* d_volume, void* str
     return launch_das(p->das, d_iq, p->iq_bf16, d_volume, (cudaStream_t)stream, &p->launches);
 }
 
+CUTB_API bool cutb_plan_check(cutb_plan* p, void* stream)
+{
+    CUTB_REQUIRE(p, CUTB_ERR_INVALID_ARGUMENT, "Null plan.");
+    int status = 0;
+    CUTB_CUDA_OK(cudaMemcpyAsync(&status, p->d_status, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    CUTB_CUDA_OK(cudaStreamSynchronize((cudaStream_t)stream));
+    if (status) {
+        CUTB_CUDA_OK(cudaMemsetAsync(p->d_status, 0, sizeof(int), (cudaStream_t)stream));
+        set_error(CUTB_ERR_TIMEOUT, "A device-side wait of the delay-and-sum kernel gave up (status %#x).", status);
+        return false;
+    }
+    return true;
+}
+
 CUTB_API bool cutb_beamform(cutb_plan* p, const void* d_raw, size_t raw_bytes, void* d_volume, void* stream)
 {
     CUTB_REQUIRE(p, CUTB_ERR_INVALID_ARGUMENT, "Null plan.");
@@ -331,6 +345,9 @@ bool cutb_plan::build(const CudaBeamformerParameters& params, const cutb_options
     vol_bytes = (size_t)bp.output_points[0] * bp.output_points[1] * bp.output_points[2] * 8;
     if (!alloc_bytes((void**)&d_decoded, samples * sizeof(float))) return false;
     if (!alloc_bytes(&d_iq, iq_bytes)) return false;
+    if (!alloc_bytes((void**)&d_status, sizeof(int))) return false;
+    CUTB_CUDA_OK(cudaMemset(d_status, 0, sizeof(int)));
+    das.status = d_status;
     return true;
 }
 
@@ -338,4 +355,5 @@ cutb_plan::~cutb_plan()
 {
     device_free(d_decoded);
     device_free(d_iq);
+    device_free(d_status);
 }

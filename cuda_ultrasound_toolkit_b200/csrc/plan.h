@@ -44,6 +44,7 @@ struct cutb_plan {
     size_t raw_bytes = 0, iq_bytes = 0, vol_bytes = 0;
     float* d_decoded = nullptr;
     void* d_iq = nullptr;
+    int* d_status = nullptr;   // device-side error word of the stage kernels
     int launches = 0;
 
     bool build(const CudaBeamformerParameters& params, const cutb_options* options);

@@ -69,6 +69,7 @@ struct DasArgs {
     float cf_power;            // coherence exponent in [0, 1]
     float to_power;            // sine apodization exponent
     unsigned long long readi_row;  // bit g set: sub-signal g negated
+    int* status;               // device word: bit 0 set when a bounded wait gave up
 };
 
 // Derives the delay-and-sum constants from the parameter block, applying the same

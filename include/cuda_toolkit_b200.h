@@ -94,6 +94,10 @@ CUTB_API bool cutb_das(cutb_plan* plan, const void* d_iq, void* d_volume, void* 
 /* Whole pipeline on device memory, intermediates in the plan's own buffers. */
 CUTB_API bool cutb_beamform(cutb_plan* plan, const void* d_raw, size_t raw_bytes, void* d_volume, void* stream);
 
+/* Synchronises `stream` and reports whether a kernel of this plan hit a bounded device-side
+ * wait (CUTB_ERR_TIMEOUT); clears the flag. cuda_toolkit::beamform calls it on every frame. */
+CUTB_API bool cutb_plan_check(cutb_plan* plan, void* stream);
+
 /* Number of kernels the last cutb_beamform/cutb_decode/cutb_hilbert/cutb_das call launched. */
 CUTB_API int cutb_plan_last_launch_count(const cutb_plan* plan);
 

@@ -335,19 +335,26 @@ int derive(const CudaBeamformerParameters& bp, Geometry& g)
     g.Y = bp.output_points[1];
     g.Z = bp.output_points[2];
     if (!g.S || !g.C || !g.T || !g.X || !g.Y || !g.Z) return -1;
-    g.spm = (double)bp.sampling_frequency / (double)bp.speed_of_sound;
+    /* The constants are FP32 values upstream (BeamformerConstants, beamformer_constants.cuh:32-72,
+     * filled by beamformer.cu:17-98 in float arithmetic); they are formed the same way here and
+     * only the per-voxel arithmetic below runs in double. */
+    const float spm = bp.sampling_frequency / bp.speed_of_sound;
+    const float hpx = bp.xdc_element_pitch[0] * 0.5f, hpy = bp.xdc_element_pitch[1] * 0.5f;
+    g.spm = spm;
     g.px = bp.xdc_element_pitch[0];
     g.py = bp.xdc_element_pitch[1];
-    g.xmin_x = -(double)bp.xdc_transform[12] + 0.5 * g.px;
-    g.xmin_y = -(double)bp.xdc_transform[13] + 0.5 * g.py;
-    g.xmax_x = (double)bp.xdc_transform[12] - 0.5 * g.px;
-    g.xmax_y = (double)bp.xdc_transform[13] - 0.5 * g.py;
+    g.xmin_x = (float)(-bp.xdc_transform[12] + hpx);
+    g.xmin_y = (float)(-bp.xdc_transform[13] + hpy);
+    g.xmax_x = (float)(bp.xdc_transform[12] - hpx);
+    g.xmax_y = (float)(bp.xdc_transform[13] - hpy);
     g.delay = (double)(int)(bp.time_offset * bp.sampling_frequency);
     for (int a = 0; a < 3; ++a) g.vmin[a] = bp.output_min_coordinate[a];
-    /* Lateral resolution is used for both x and y (beamformer.cu:42-49); a single point has step 0. */
-    g.res[0] = g.X > 1 ? ((double)bp.output_max_coordinate[0] - bp.output_min_coordinate[0]) / (g.X - 1) : 0.0;
-    g.res[1] = g.res[0];
-    g.res[2] = g.Z > 1 ? ((double)bp.output_max_coordinate[2] - bp.output_min_coordinate[2]) / (g.Z - 1) : 0.0;
+    /* Lateral step is used for both x and y (beamformer.cu:42-49); a single point has step 0. */
+    const float rx = g.X > 1 ? (bp.output_max_coordinate[0] - bp.output_min_coordinate[0]) / (float)(g.X - 1) : 0.f;
+    const float rz = g.Z > 1 ? (bp.output_max_coordinate[2] - bp.output_min_coordinate[2]) / (float)(g.Z - 1) : 0.f;
+    g.res[0] = rx;
+    g.res[1] = rx;
+    g.res[2] = rz;
     g.fy = bp.foci[1];
     g.fz = bp.foci[2];
     g.seq = bp.das_shader_id;

@@ -109,7 +109,7 @@ def test_hilbert_vs_fp64(torch, orc, N, taps):
     T, C = 3, 5                                    # 15 rows: odd count exercises the unpaired row
     rng = np.random.default_rng(N + taps)
     rows = rng.normal(size=(T, C, N)).astype(np.float32)
-    bp = base_params(N, C, T)
+    bp = base_params(N, C, T, decode=EncodingMatrix.NONE)
     h = None
     if taps:
         h = synth.chirp_taps(min(taps, N))
