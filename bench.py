@@ -44,6 +44,23 @@ def workload_config(extra=None):
     return cfg
 
 
+# ---- frame-parallel sharding ------------------------------------------------------------------------
+def frame_seeds(rank, world, per_rank=2, base=7000):
+    """Seeds of the frames rank `rank` beamforms: disjoint across ranks, fixed per rank (weak scaling)."""
+    return [base + per_rank * rank + k for k in range(per_rank)]
+
+
+def max_over_ranks(values, world, device=None):
+    """Element-wise max of per-rank timings (the job is as slow as its slowest rank)."""
+    if world <= 1:
+        return list(values)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 # ---- clocks sampled during the timed region ------------------------------------------------------
 class ClockSampler:
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -176,7 +193,7 @@ def run_ours(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    frames = [synth.frame(WORKLOAD, seed=7000 + 2 * rank + k) for k in range(2)]
+    frames = [synth.frame(WORKLOAD, seed=sd) for sd in frame_seeds(rank, world)]
     bp = frames[0][1]
     for _, b in frames[1:]:  # same geometry; only the data and channel map differ per frame
         assert b.dims == bp.dims
@@ -248,10 +265,7 @@ def run_ours(args, rank, world, local_rank):
     barrier()
 
     # Max over ranks.
-    if world > 1:
-        t = torch.tensor([ms, e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_s = t.tolist()
+    ms, e2e_s = max_over_ranks([ms, e2e_s], world, dev)
     if rank != 0:
         return
 
