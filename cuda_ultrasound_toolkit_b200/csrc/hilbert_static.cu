@@ -1,0 +1,89 @@
+// cutb_hilbert_static: the match-filtered analytic signal without any device allocation.
+//
+// Who needs it: applications that own the GPU's memory budget themselves, such as an
+// acquisition loop that reserves every buffer it will use before scanning starts, or a
+// plugin host that only lends the library its own buffers. They cannot let a library call
+// cudaMalloc/cudaFree: those calls can stall on device-wide synchronisation in the middle of
+// a frame, and they fail once the host has reserved the memory. cutb_hilbert needs a plan,
+// and creating a plan allocates the twiddle and spectral-weight tables that the kernel reads.
+// This entry point keeps those tables in a fixed file-scope device array instead, so every
+// byte it touches is either the caller's input/output or that array.
+//
+// The array holds the tables of one transform of up to kStaticMaxSamples samples per row
+// (384 KiB); every GPU that loads the library keeps it until the process exits. Each call
+// rewrites all the tables it needs, on the caller's stream, before the kernel reads them, so
+// nothing in the array has to start at zero. All calls share the array: calls that overlap
+// on the GPU (on different streams, or issued from several host threads) race on it and must
+// be serialised by the caller.
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+#include "stages.h"
+
+namespace cutb {
+namespace {
+
+constexpr unsigned kStaticMaxSamples = 16384;
+constexpr int kMaxDevices = 64;
+
+// twiddle | Ge | Go, kStaticMaxSamples complex values each.
+static __device__ __align__(256) float g_hilbert_tables[3 * 2 * kStaticMaxSamples];
+
+std::mutex g_setup_mutex;
+float* g_table_address[kMaxDevices] = {};
+
+// Device address of the table array on the current device. In host code the name
+// g_hilbert_tables is only a handle for the runtime, not an address the kernel may use; the
+// address is looked up once per device, with that device current.
+bool table_address(float** out)
+{
+    int dev = 0;
+    CUTB_CUDA_OK(cudaGetDevice(&dev));
+    CUTB_REQUIRE(dev >= 0 && dev < kMaxDevices, CUTB_ERR_UNSUPPORTED, "Device index %d too large.", dev);
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (!g_table_address[dev]) {
+        void* p = nullptr;
+        CUTB_CUDA_OK(cudaGetSymbolAddress(&p, g_hilbert_tables));
+        g_table_address[dev] = static_cast<float*>(p);
+    }
+    *out = g_table_address[dev];
+    return true;
+}
+
+}  // namespace
+}  // namespace cutb
+
+using namespace cutb;
+
+extern "C" CUTB_API bool cutb_hilbert_static(const float* d_in, uint in_stride, void* d_iq, uint samples,
+                                             size_t rows, const float* taps, uint ntaps, void* stream)
+{
+    CUTB_REQUIRE(d_in && d_iq, CUTB_ERR_INVALID_ARGUMENT, "cutb_hilbert_static: null device buffer.");
+    CUTB_REQUIRE(in_stride == 1 || in_stride == 2, CUTB_ERR_INVALID_ARGUMENT, "Input stride must be 1 or 2.");
+    CUTB_REQUIRE(rows > 0, CUTB_ERR_INVALID_ARGUMENT, "cutb_hilbert_static: no rows.");
+    CUTB_REQUIRE(samples <= kStaticMaxSamples, CUTB_ERR_INVALID_ARGUMENT,
+                 "cutb_hilbert_static: %u samples per row exceed the fixed table capacity of %u.", samples,
+                 kStaticMaxSamples);
+    CUTB_REQUIRE(hilbert_supported_length(samples), CUTB_ERR_UNSUPPORTED,
+                 "Sample count %u not supported by the FFT (powers of two 16..%u).", samples, kMaxHilbertLength);
+    CUTB_REQUIRE(ntaps == 0 || taps, CUTB_ERR_INVALID_ARGUMENT, "Null match filter.");
+    std::vector<float> tw, ge, go;  // host memory only
+    if (!build_hilbert_tables(samples, taps, ntaps, tw, ge, go)) return false;
+    float* tables = nullptr;
+    if (!table_address(&tables)) return false;
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t n = 2 * (size_t)samples;
+    CUTB_CUDA_OK(cudaMemcpyAsync(tables, tw.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
+    CUTB_CUDA_OK(cudaMemcpyAsync(tables + n, ge.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
+    CUTB_CUDA_OK(cudaMemcpyAsync(tables + 2 * n, go.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
+    HilbertArgs a{};
+    a.rows = rows;
+    a.log_n = 0;
+    while ((1u << a.log_n) < samples) ++a.log_n;
+    a.in_stride = in_stride;
+    a.twiddle = tables;
+    a.ge = tables + n;
+    a.go = tables + 2 * n;
+    return launch_hilbert(a, d_in, d_iq, false, st);
+}

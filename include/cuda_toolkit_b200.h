@@ -101,6 +101,20 @@ CUTB_API bool cutb_plan_check(cutb_plan* plan, void* stream);
 /* Number of kernels the last cutb_beamform/cutb_decode/cutb_hilbert/cutb_das call launched. */
 CUTB_API int cutb_plan_last_launch_count(const cutb_plan* plan);
 
+/* No counterpart in the upstream library. The analytic signal of cutb_hilbert for callers that
+ * cannot let a library allocate device memory: applications that own the GPU memory budget (an
+ * acquisition loop that reserves its buffers up front, a plugin host that lends its buffers),
+ * where cudaMalloc/cudaFree could stall on device-wide synchronisation mid-frame or fail once the
+ * host has reserved the memory. No plan and no allocation: d_in holds rows x samples floats with
+ * element stride in_stride (1 or 2), d_iq receives rows x samples complex64, taps/ntaps is the
+ * match filter in host memory (ntaps <= samples, 0 = none). The FFT tables live in a fixed device
+ * array sized for samples <= 16384 (384 KiB, held by every GPU that loads the library until the
+ * process exits); longer rows are rejected with CUTB_ERR_INVALID_ARGUMENT. The first call on a
+ * device looks up that array's address, so make it before any stream capture. Every call rewrites
+ * the array on `stream`; calls that overlap on the GPU race on it and must be serialised. */
+CUTB_API bool cutb_hilbert_static(const float* d_in, uint in_stride, void* d_iq, uint samples, size_t rows,
+                                  const float* taps, uint ntaps, void* stream);
+
 /* Measures the device's FP32 fused-multiply-add throughput (TFLOP/s) with a short
  * register-only kernel on `stream`; the roofline denominator of the delay-and-sum stage. */
 CUTB_API bool cutb_calibrate_fp32(double* tflops, void* stream);

@@ -1,0 +1,70 @@
+"""cutb_hilbert_static: the analytic signal for callers that cannot let the library allocate.
+
+Applications that own the GPU memory budget (an acquisition loop that reserves all its buffers
+before scanning, a plugin host that lends the library its own buffers) need a call that makes no
+device allocation: cudaMalloc/cudaFree can stall on device-wide synchronisation mid-frame, and
+they fail once the host has reserved the memory. cutb_hilbert_static keeps its FFT tables in a
+fixed device array instead of a plan. This test calls it through the C ABI and checks it against
+the plan-based entry point cutb_hilbert, on two calls in a row that rewrite the shared array with
+different sizes and filters. The file is named to be collected last.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from cuda_ultrasound_toolkit_b200 import EncodingMatrix, Plan, lib, synth
+
+pytestmark = pytest.mark.gpu
+
+TOL_HILBERT = 2e-6  # the relative-L2 bar of the other Hilbert parity tests
+
+
+def _static_entry():
+    fn = lib().cutb_hilbert_static
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p, ctypes.c_uint, ctypes.c_size_t,
+                   ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p]
+    fn.restype = ctypes.c_bool
+    return fn
+
+
+def _plan(S, C, T, taps):
+    w = synth.Workload("static", T, C, S, 8, 8, 8, 0, cubic=True, cf=0.0, encoding=EncodingMatrix.NONE)
+    bp = synth.make_params(w)
+    bp.filter_length = len(taps)
+    for i, v in enumerate(taps):
+        bp.rf_filter[i] = float(v)
+    return Plan(bp)
+
+
+def test_static_hilbert_matches_plan_entry_point():
+    import torch
+    fn = _static_entry()
+    stream = torch.cuda.current_stream()
+    rng = np.random.default_rng(11)
+    # Two calls in a row with different lengths, filters and input strides.
+    for S, C, T, taps, stride in [(4096, 5, 3, synth.chirp_taps(64), 1), (1024, 4, 2, synth.chirp_taps(17), 2)]:
+        rows = rng.normal(size=(T, C, S)).astype(np.float32)
+        d_rows = torch.from_numpy(rows).cuda()
+        want = _plan(S, C, T, taps).hilbert(d_rows).cpu().numpy()
+        if stride == 2:
+            src = torch.zeros((T, C, S, 2), dtype=torch.float32, device="cuda")
+            src[..., 0] = d_rows
+        else:
+            src = d_rows
+        out = torch.full((T, C, S), 99 + 99j, dtype=torch.complex64, device="cuda")
+        t = np.ascontiguousarray(taps, dtype=np.float32)
+        assert fn(src.data_ptr(), stride, out.data_ptr(), S, T * C, t.ctypes.data, len(t),
+                  ctypes.c_void_p(stream.cuda_stream))
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        err = np.linalg.norm(got - want) / np.linalg.norm(want)
+        assert err < TOL_HILBERT, err
+
+
+def test_static_hilbert_rejects_rows_beyond_capacity():
+    import torch
+    fn = _static_entry()
+    buf = torch.zeros(16, dtype=torch.float32, device="cuda")
+    assert not fn(buf.data_ptr(), 1, buf.data_ptr(), 32768, 1, None, 0, None)
+    assert lib().cutb_last_error() == 1
