@@ -193,7 +193,11 @@ def run_ours(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    frames = [synth.frame(WORKLOAD, seed=sd) for sd in frame_seeds(rank, world)]
+    # Frames of one acquisition: same probe set-up (channel map), different echoes.
+    seeds = frame_seeds(rank, world)
+    frames = [synth.frame(WORKLOAD, seed=seeds[0])]
+    cmap = np.ctypeslib.as_array(frames[0][1].channel_mapping)[: frames[0][1].dims[1]].copy()
+    frames += [synth.frame(WORKLOAD, seed=sd, channel_map=cmap) for sd in seeds[1:]]
     bp = frames[0][1]
     for _, b in frames[1:]:  # same geometry; only the data and channel map differ per frame
         assert b.dims == bp.dims

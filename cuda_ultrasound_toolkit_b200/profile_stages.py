@@ -1,0 +1,36 @@
+"""Runs each pipeline stage once on a synthetic frame, for profilers.
+
+    python -m cuda_ultrasound_toolkit_b200.profile_stages [--workload full] [--repeat 1]
+
+Launch order: one warm-up pass of decode, Hilbert, delay-and-sum (3 kernels), then `repeat`
+passes of the same three kernels. With ncu, skip the warm-up with `-s 3`.
+"""
+import argparse
+
+import torch
+
+from . import Plan, synth
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="full", choices=sorted(synth.CONFIGS))
+    ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--bf16", action="store_true", help="store the analytic signal as bf16")
+    args = ap.parse_args()
+    raw, bp = synth.frame(args.workload)
+    plan = Plan(bp, iq_bf16=args.bf16)
+    d_raw = torch.from_numpy(raw).cuda()
+    vol, dec, iq = plan.empty_volume(), plan.empty_decoded(), plan.empty_iq()
+    plan.beamform(d_raw, out=vol)
+    for _ in range(args.repeat):
+        plan.decode(d_raw, out=dec)
+        plan.hilbert(dec, out=iq)
+        plan.das(iq, out=vol)
+    plan.check()
+    torch.cuda.synchronize()
+    print(f"ok: {args.workload}, {3 * (args.repeat + 1)} kernels")
+
+
+if __name__ == "__main__":
+    main()

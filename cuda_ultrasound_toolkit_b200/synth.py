@@ -158,8 +158,9 @@ def echoes(w: Workload, pos, amp, half_width=16):
     return out.reshape(T, C, S)
 
 
-def synth_frame(w: Workload, seed: int):
-    """Returns (raw int16 [C][T*S], channel_map, scatterer positions, amplitudes)."""
+def synth_frame(w: Workload, seed: int, channel_map=None):
+    """Returns (raw int16 [C][T*S], channel_map, scatterer positions, amplitudes).
+    channel_map: raw channel of each receive channel; a seeded permutation when None."""
     rng = np.random.default_rng(seed)
     pos, amp = scatterer_field(w, rng)
     e = echoes(w, pos, amp)
@@ -173,17 +174,19 @@ def synth_frame(w: Workload, seed: int):
     enc *= 0.8 * 32767 / np.max(np.abs(enc))
     q = np.rint(enc).astype(np.int16).reshape(T, C, S)
     cmap = rng.permutation(C).astype(np.int16)
+    if channel_map is not None:
+        cmap = np.asarray(channel_map, dtype=np.int16)
     raw = np.empty((C, T, S), dtype=np.int16)
     raw[cmap] = q.transpose(1, 0, 2)
     return raw.reshape(C, T * S), cmap, pos, amp
 
 
-def frame(name: str, seed: int = None, data_type=InputDataTypes.TYPE_I16):
+def frame(name: str, seed: int = None, data_type=InputDataTypes.TYPE_I16, channel_map=None):
     """(raw, params) for a named configuration; seed defaults to a fixed per-config value."""
     w = CONFIGS[name]
     if seed is None:
         seed = 1000 * (list(CONFIGS).index(name) + 1)
-    raw, cmap, _, _ = synth_frame(w, seed)
+    raw, cmap, _, _ = synth_frame(w, seed, channel_map)
     bp = make_params(w, data_type=data_type, channel_map=cmap)
     if data_type == InputDataTypes.TYPE_F32:
         raw = raw.astype(np.float32)
