@@ -79,7 +79,8 @@ bool build_encoding(unsigned n, int ordering, EncodingInfo& info)
             }
 
     // Output row k holds natural row order[k]. WALSH sorts rows by their number of sign
-    // changes; equal counts (possible only with the 12/20 bases) keep natural order.
+    // changes with std::sort and upstream's comparator (hadamard_decoder.cpp:209-211), so rows
+    // with equal counts (possible only with the 12/20 bases) land where upstream puts them.
     std::vector<unsigned> order(n);
     std::iota(order.begin(), order.end(), 0u);
     if (ordering == WALSH) {
@@ -87,7 +88,7 @@ bool build_encoding(unsigned n, int ordering, EncodingInfo& info)
         for (unsigned r = 0; r < n; ++r)
             for (unsigned c = 0; c + 1 < n; ++c)
                 flips[r] += (h[(size_t)r * n + c] * h[(size_t)r * n + c + 1]) < 0;
-        std::stable_sort(order.begin(), order.end(), [&](unsigned x, unsigned y) { return flips[x] < flips[y]; });
+        std::sort(order.begin(), order.end(), [&](unsigned x, unsigned y) { return flips[x] < flips[y]; });
     }
 
     info.n = n;

@@ -11,12 +11,12 @@
  * upstream file:line it follows (paths relative to the upstream repository
  * root, cuda_toolkit/src/...).
  *
- * Pinning: the upstream repository ships no tests, golden vectors or known-answer
- * tests. This restatement is pinned by (1) closed-form known answers
- * (H*H^T = N*I, decode(H*x) == x, the analytic signal of a pure cosine, the
- * focus of a point scatterer) and (2) the golden fixtures under tests/golden/,
- * which were produced by compiling the upstream sources themselves
- * (oracle/ref_harness.cpp + oracle/Makefile) and running them on the CPU.
+ * Pinning: the upstream repository ships no tests, golden vectors or known-answer tests. This
+ * restatement is pinned by (1) closed-form known answers (H*H^T = N*I, decode(H^T x) == x, the
+ * analytic signal of pure cosines, the focus of a point scatterer, linearity) and (2) the golden
+ * fixtures under tests/golden/, produced by upstream's own code: its sources compiled unmodified
+ * for the CPU (oracle/Makefile.ref, CUDA/cuBLAS/cuFFT emulated by oracle/ref_shim/) and driven
+ * through its entry points by tests/golden/make_golden.py.
  *
  * Threads: std::thread over rows / voxels; nthreads <= 0 uses every host core.
  */
@@ -97,7 +97,7 @@ extern "C" {
  * Encoding matrix of order n, row-major +-1 (hadamard_decoder.cpp:110-189, 191-222).
  * Sylvester doubling [[H, H], [H, -H]] from a base of order 1 (n = 2^k), 12 (n = 12*2^k)
  * or 20 (n = 20*2^k). ordering == 2 (WALSH) reorders the rows by their number of sign
- * changes (ties keep their natural order). Returns 0, or -1 for an unsupported order.
+ * changes. Returns 0, or -1 for an unsupported order.
  */
 int orc_encoding_matrix(unsigned n, int ordering, signed char* out)
 {
@@ -126,8 +126,10 @@ int orc_encoding_matrix(unsigned n, int ordering, signed char* out)
         for (unsigned r = 0; r < n; ++r)
             for (unsigned c = 0; c + 1 < n; ++c)
                 flips[r] += h[(size_t)r * n + c] * h[(size_t)r * n + c + 1] < 0;
-        std::stable_sort(order.begin(), order.end(),
-                         [&](unsigned a, unsigned bb) { return flips[a] < flips[bb]; });
+        /* std::sort with upstream's comparator (hadamard_decoder.cpp:209-211): ties between rows
+         * of equal sign-change count (possible with the 12/20 bases) are ordered as upstream's
+         * sort orders them with the same C++ standard library. */
+        std::sort(order.begin(), order.end(), [&](unsigned a, unsigned bb) { return flips[a] < flips[bb]; });
     }
     for (unsigned r = 0; r < n; ++r)
         for (unsigned c = 0; c < n; ++c) out[(size_t)r * n + c] = (signed char)h[(size_t)order[r] * n + c];
