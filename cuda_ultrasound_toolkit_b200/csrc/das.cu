@@ -91,19 +91,6 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
-__device__ __forceinline__ float approx_sqrt(float x)
-{
-    float r;
-    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
-__device__ __forceinline__ float approx_rcp(float x)
-{
-    float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
-
 // f-number Hann window, beamformer_utils.cuh:142-154.
 __device__ __forceinline__ float hann_apo(float lateral, float depth, float fnum)
 {
