@@ -47,6 +47,7 @@ constexpr int kRows = 8;          // rows (channels) per stage
 constexpr int kStages = 3;        // raw stage buffers in flight
 constexpr int kWinMax = 136;      // samples per staged window
 constexpr int kBatch = 8;         // stages whose window metadata is computed together
+constexpr int kSlots = 2 * kBatch;  // metadata ring: a batch never overwrites a stage still being issued
 constexpr float kPi = 3.141592654f;  // value of CUDART_PI_F used upstream
 constexpr long long kWaitLimitCycles = 400000000ll;  // ~0.2 s at 2 GHz
 
@@ -176,9 +177,9 @@ struct alignas(128) Smem {
     RowMeta rowc[CUBIC ? kRows : 1];  // metadata of the rows whose coefficients are built
     RowMeta row[kStages][kRows];
     StageMeta stage[kStages];
-    RowMeta next_row[kBatch][kRows];    // precomputed metadata of the next kBatch stages
-    StageMeta next_stage[kBatch];
-    int next_bytes[kBatch][kRows];
+    RowMeta next_row[kSlots][kRows];    // precomputed metadata of upcoming stages (ring)
+    StageMeta next_stage[kSlots];
+    int next_bytes[kSlots][kRows];
     uint64_t full[kStages];
     int abort;
     int tx_reach_bits;
@@ -324,7 +325,7 @@ __device__ __forceinline__ void compute_batch(Smem<IQ, CUBIC>& sm, int first, in
 {
     for (int i = threadIdx.x; i < kBatch * kRows; i += kThreads) {
         const int k = first + i / kRows;
-        if (k < nstages) compute_row<SEQ>(sm, (k % kBatch), stage_id(a, k, nchunks), i % kRows, a, tile);
+        if (k < nstages) compute_row<SEQ>(sm, (k % kSlots), stage_id(a, k, nchunks), i % kRows, a, tile);
     }
 }
 
@@ -333,7 +334,7 @@ template <class IQ, bool CUBIC>
 __device__ __forceinline__ void issue_row(Smem<IQ, CUBIC>& sm, int b, int k, int q, const DasArgs& a,
                                           const IQ* __restrict__ iq)
 {
-    const int slot = k % kBatch;
+    const int slot = k % kSlots;
     const StageMeta& st = sm.next_stage[slot];
     const RowMeta m = sm.next_row[slot][q];
     const unsigned bytes = (unsigned)sm.next_bytes[slot][q];
@@ -450,21 +451,26 @@ __device__ __forceinline__ void row_pass(const DasArgs& a, const Smem<IQ, CUBIC_
 // Thread layout. HERCULES: lanes are 4 (x) x 8 (y) neighbours, whose delays differ by less
 // than a sample or two, so their shared-memory reads fall in distinct banks or broadcast;
 // warps and the kVpt registers of a thread run along z. FORCES (no y): lanes along x.
-template <int SEQ>
+template <int SEQ, bool SHORT>
 struct Layout {
-    static constexpr int TX = SEQ == HERCULES ? 4 : 32;
+    // HERCULES: lanes cover 4 (x) x 8 (y) voxels, each thread kVpt consecutive depths; the
+    // four warps stack along z (4 x 8 x 32), or, for SHORT tiles, two along x and two along z
+    // (8 x 8 x 16) -- the short tile halves the depth span, and with it the staged window,
+    // when the z step is coarse. FORCES: lanes along x (32 x 1 x 32).
+    static constexpr bool kShort = SEQ == HERCULES && SHORT;
+    static constexpr int TX = SEQ == HERCULES ? (kShort ? 8 : 4) : 32;
     static constexpr int TY = SEQ == HERCULES ? 8 : 1;
-    static constexpr int TZ = kWarps * kVpt;
+    static constexpr int TZ = (kShort ? 2 : kWarps) * kVpt;
 };
 
-template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ>
+template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT>
 __global__ void __launch_bounds__(kThreads, 3)
 das_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     auto& sm = *reinterpret_cast<Smem<IQ, CUBIC>*>(smem_raw);
     constexpr bool HERC = SEQ == HERCULES;
-    using L = Layout<SEQ>;
+    using L = Layout<SEQ, SHORT>;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
     // ---- tile, voxels, offsets from the tile centre -----------------------------------------
@@ -480,9 +486,9 @@ das_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
         const double hz = 0.5 * (L::TZ - 1) * fabs((double)a.res_z);
         tile.radius = (float)(sqrt(hx * hx + hy * hy + hz * hz) * (1.0 + 1e-6) + 1e-9);
     }
-    const int x_idx = tx0 + (HERC ? (lane & 3) : lane);
+    const int x_idx = tx0 + (HERC ? (L::kShort ? 4 * (warp & 1) : 0) + (lane & 3) : lane);
     const int y_idx = HERC ? ty0 + (lane >> 2) : 0;
-    const int z_first = tz0 + warp * kVpt;
+    const int z_first = tz0 + (L::kShort ? (warp >> 1) : warp) * kVpt;
     // Offsets in voxel units are exact in FP32; scaled by the step they carry one rounding.
     const float dxe = ((float)x_idx - ix_c) * a.res_x;
     const float dye = HERC ? ((float)y_idx - iy_c) * a.res_y : 0.f;
@@ -626,13 +632,13 @@ das_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
     }
 }
 
-template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ>
+template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT>
 bool launch_das_t(const DasArgs& a, const void* iq, void* volume, cudaStream_t st)
 {
-    using L = Layout<SEQ>;
+    using L = Layout<SEQ, SHORT>;
     const dim3 grid(div_up(a.X, L::TX), div_up(a.Y, L::TY), div_up(a.Z, L::TZ));
     CUTB_REQUIRE(grid.y <= 65535 && grid.z <= 65535, CUTB_ERR_UNSUPPORTED, "Output grid too large.");
-    auto kern = das_kernel<SEQ, CUBIC, CF, APO, IQ>;
+    auto kern = das_kernel<SEQ, CUBIC, CF, APO, IQ, SHORT>;
     const size_t smem = sizeof(Smem<IQ, CUBIC>);
     static bool configured = false;
     if (!configured) {
@@ -644,12 +650,23 @@ bool launch_das_t(const DasArgs& a, const void* iq, void* volume, cudaStream_t s
     return true;
 }
 
-template <int SEQ, class IQ>
+// True when the 4 x 8 x 32 HERCULES tile's staged window (twice the largest index move over
+// the tile, receive and transmit path each 1-Lipschitz, plus the interpolation taps) would not
+// fit the stage buffers, so that the 8 x 8 x 16 tile is used.
+bool prefer_short_tile(const DasArgs& a)
+{
+    const double hx = 1.5 * std::fabs((double)a.res_x), hy = 3.5 * std::fabs((double)a.res_y);
+    const double hz = 15.5 * std::fabs((double)a.res_z);
+    const double reach = std::sqrt(hx * hx + hy * hy + hz * hz) * (double)a.spm;
+    return 4.0 * reach + 8.0 > (double)(kWinMax - 8);
+}
+
+template <int SEQ, class IQ, bool SHORT>
 bool launch_das_s(const DasArgs& a, const void* iq, void* volume, cudaStream_t st)
 {
 #define CUTB_DAS_CASE(CUBIC, CF, APO)                                                   \
     if ((bool)a.cubic == CUBIC && (bool)a.apply_cf == CF && (bool)a.use_apo == APO) \
-        return launch_das_t<SEQ, CUBIC, CF, APO, IQ>(a, iq, volume, st);
+        return launch_das_t<SEQ, CUBIC, CF, APO, IQ, SHORT>(a, iq, volume, st);
     CUTB_DAS_CASE(true, true, false)
     CUTB_DAS_CASE(true, false, false)
     CUTB_DAS_CASE(false, true, false)
@@ -771,12 +788,15 @@ bool launch_das(const DasArgs& a, const void* iq, bool iq_bf16, void* volume, cu
     CUTB_REQUIRE(a.S % 4 == 0, CUTB_ERR_UNSUPPORTED,
                  "Delay-and-sum needs a sample count that is a multiple of 4 (got %d).", a.S);
     bool ok;
-    if (a.seq == HERCULES)
-        ok = iq_bf16 ? launch_das_s<HERCULES, __nv_bfloat162>(a, iq, volume, st)
-                     : launch_das_s<HERCULES, float2>(a, iq, volume, st);
+    if (a.seq == HERCULES && (a.tile == 2 || (a.tile == 0 && prefer_short_tile(a))))
+        ok = iq_bf16 ? launch_das_s<HERCULES, __nv_bfloat162, true>(a, iq, volume, st)
+                     : launch_das_s<HERCULES, float2, true>(a, iq, volume, st);
+    else if (a.seq == HERCULES)
+        ok = iq_bf16 ? launch_das_s<HERCULES, __nv_bfloat162, false>(a, iq, volume, st)
+                     : launch_das_s<HERCULES, float2, false>(a, iq, volume, st);
     else
-        ok = iq_bf16 ? launch_das_s<FORCES, __nv_bfloat162>(a, iq, volume, st)
-                     : launch_das_s<FORCES, float2>(a, iq, volume, st);
+        ok = iq_bf16 ? launch_das_s<FORCES, __nv_bfloat162, false>(a, iq, volume, st)
+                     : launch_das_s<FORCES, float2, false>(a, iq, volume, st);
     if (ok && launches) ++*launches;
     return ok;
 }

@@ -337,6 +337,9 @@ bool cutb_plan::build(const CudaBeamformerParameters& params, const cutb_options
                  bp.filter_length, MAX_FILTER_LENGTH);
     if (!fe.set_filter(bp.rf_filter, bp.filter_length)) return false;
     if (!derive_das(bp, das)) return false;
+    CUTB_REQUIRE(opt.das_tile >= 0 && opt.das_tile <= 2, CUTB_ERR_INVALID_ARGUMENT, "Unknown tile id %d.",
+                 opt.das_tile);
+    das.tile = opt.das_tile;
 
     const size_t esize = data_type == TYPE_I16 ? 2 : 4;
     raw_bytes = (size_t)bp.rf_raw_dim[0] * bp.rf_raw_dim[1] * esize;

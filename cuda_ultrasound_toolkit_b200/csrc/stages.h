@@ -69,6 +69,7 @@ struct DasArgs {
     float cf_power;            // coherence exponent in [0, 1]
     float to_power;            // sine apodization exponent
     unsigned long long readi_row;  // bit g set: sub-signal g negated
+    int tile;                  // HERCULES tile: 0 chosen from the grid, 1 = 4 x 8 x 32, 2 = 8 x 8 x 16
     int* status;               // device word: bit 0 set when a bounded wait gave up
 };
 

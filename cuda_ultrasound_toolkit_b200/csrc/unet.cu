@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "../../include/cuda_toolkit_b200_learn.h"
 #include "conv3d.h"
 
 namespace cutb {

@@ -1,0 +1,258 @@
+"""The learned sparse-transmit path: beamform a 4x sparser transmit acquisition, restore it with
+the U-Net (csrc/unet.cu, trained by the library's own tcgen05 kernels), and gate every volume
+with an online NRMSE estimate against the plain full-transmit delay-and-sum, falling back to
+the full-transmit volume when the estimate exceeds the bar.
+
+Acquisitions (row-column array, 128 receive columns, 4096 samples, fs 20 MHz, pitch 0.3 mm):
+  full    128 transmit events, one row each, order-128 Hadamard encoding
+  sparse   32 transmit events, 4 adjacent rows fired together (a 1.2 mm virtual element),
+           order-32 Hadamard encoding
+Both are beamformed by the plain pipeline (decode + Hilbert + delay-and-sum, cubic
+interpolation, no coherence factor) onto the same 128^3 grid over x, y in [-9, 9] mm and
+z in [10, 40] mm, and divided by the simulator's gain, so volumes are in scatterer units.
+
+Phantoms: 50-400 point scatterers with U(0.5, 1) amplitudes plus 20 000 speckle scatterers
+with N(0, 0.05) amplitudes, uniform in the box; phantom k is seeded by k.
+
+NRMSE = ||V_hat - V|| / ||V|| over the complex volume, V the plain full-transmit volume.
+Gate: the full-transmit delay-and-sum on the 32^3 sub-grid of every 4th voxel (1/64 of the
+voxels) estimates the NRMSE of the restored volume; above 2 % the volume falls back to the
+full-transmit delay-and-sum, whose cost is charged to the learned path.
+
+  python -m cuda_ultrasound_toolkit_b200.sparse train --phantoms 2048 --epochs 4 --out weights.npz
+  python -m cuda_ultrasound_toolkit_b200.sparse evaluate --weights weights.npz --phantoms 256
+"""
+import argparse
+import json
+import math
+import os
+import time
+
+import numpy as np
+import torch
+
+from . import learn, synth
+from .api import Plan
+from .simulate import Simulator
+
+C, S = 128, 4096
+FULL_T, SPARSE_T, GROUP = 128, 32, 4
+GRID = (128, 128, 128)            # Z, Y, X
+BOX_XY, Z_RANGE = 9e-3, (10e-3, 40e-3)
+N_SPECKLE = 20000
+NRMSE_BAR = 0.02
+SUB = 4                           # gate sub-grid stride
+TRAIN_SEED0, EVAL_SEED0 = 0, 1_000_000
+CHANNEL_MAP = np.arange(C, dtype=np.int16)
+WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "unet_sparse4.npz")
+
+
+def acquisition_params(T, G, grid=GRID, sub=1):
+    """Pipeline parameters for T transmit events of G rows; sub > 1 gives the gate's sub-grid."""
+    Z, Y, X = grid
+    w = synth.Workload("sparse" if G > 1 else "full", T, C, S, X // sub, Y // sub, Z // sub, 0, cubic=True, cf=0.0,
+                       box_xy=BOX_XY, z_range=Z_RANGE)
+    bp = synth.make_params(w, channel_map=CHANNEL_MAP)
+    bp.xdc_element_pitch[1] = G * synth.PITCH
+    bp.xdc_transform[13] = T * G * synth.PITCH / 2
+    if sub > 1:
+        rx = 2 * BOX_XY / (X - 1)
+        rz = (Z_RANGE[1] - Z_RANGE[0]) / (Z - 1)
+        bp.output_max_coordinate[0] = -BOX_XY + (X - sub) * rx
+        bp.output_max_coordinate[1] = -BOX_XY + (Y - sub) * rx
+        bp.output_max_coordinate[2] = Z_RANGE[0] + (Z - sub) * rz
+    return bp
+
+
+def phantom(seed):
+    rng = np.random.default_rng(seed)
+    return synth.phantom(rng, int(rng.integers(50, 401)), N_SPECKLE, box_xy=BOX_XY, z_range=Z_RANGE)
+
+
+class Acquisition:
+    """Simulator + pipeline for one transmit scheme; volumes in scatterer units."""
+
+    def __init__(self, T, G, sub=1):
+        self.sim = Simulator(T, C, S, rows_per_transmit=G)
+        self.plan = Plan(acquisition_params(T, G, sub=sub))
+        self.raw = torch.empty((C, T * S), dtype=torch.int16, device="cuda")
+        self.gain = torch.empty(1, dtype=torch.float32, device="cuda")
+
+    def acquire(self, scat, seed):
+        self.sim.run(scat, CHANNEL_MAP, seed, raw=self.raw, gain=self.gain)
+        return self.raw
+
+    def volume(self, out=None):
+        out = self.plan.beamform(self.raw, out=out)
+        out /= self.gain
+        return out
+
+
+def nrmse(est, ref):
+    return float(torch.linalg.vector_norm(est - ref) / torch.linalg.vector_norm(ref))
+
+
+def make_pairs(n, seed0, log=print):
+    """(sparse volumes, full volumes) for phantoms seed0 .. seed0 + n - 1, complex64 on the GPU."""
+    Z, Y, X = GRID
+    xs = torch.empty((n, Z, Y, X), dtype=torch.complex64, device="cuda")
+    ys = torch.empty_like(xs)
+    full, sparse = Acquisition(FULL_T, 1), Acquisition(SPARSE_T, GROUP)
+    t0 = time.time()
+    for k in range(n):
+        scat = torch.from_numpy(phantom(seed0 + k)).cuda()
+        full.acquire(scat, 2 * (seed0 + k))
+        full.volume(out=ys[k])
+        sparse.acquire(scat, 2 * (seed0 + k) + 1)
+        sparse.volume(out=xs[k])
+        if (k + 1) % 256 == 0:
+            torch.cuda.synchronize()
+            log(f"pairs {k + 1}/{n} {time.time() - t0:.1f}s")
+    full.plan.check()
+    sparse.plan.check()
+    return xs, ys
+
+
+def train(args, log=print):
+    torch.manual_seed(0)
+    xs, ys = make_pairs(args.phantoms, TRAIN_SEED0, log)
+    net = learn.UNet(GRID, max_batch=args.batch, seed=args.seed)
+    steps = args.epochs * (args.phantoms // args.batch)
+    gen = torch.Generator(device="cpu").manual_seed(args.seed)
+    t0, step, hist = time.time(), 0, []
+    for ep in range(args.epochs):
+        perm = torch.randperm(args.phantoms, generator=gen)
+        for b in range(args.phantoms // args.batch):
+            idx = perm[b * args.batch:(b + 1) * args.batch].cuda()
+            lr = args.lr * 0.5 * (1 + math.cos(math.pi * step / steps))
+            net.train_step(xs.index_select(0, idx), ys.index_select(0, idx), lr)
+            step += 1
+            if step % 200 == 0 or step == steps:
+                loss = net.last_loss()
+                hist.append((step, loss))
+                log(f"epoch {ep} step {step}/{steps} loss {loss:.5f} {time.time() - t0:.1f}s")
+    torch.cuda.synchronize()
+    train_s = time.time() - t0
+    params = net.get_params()
+    np.savez_compressed(args.out, params=params, grid=np.array(GRID), phantoms=args.phantoms, epochs=args.epochs,
+                        batch=args.batch, lr=args.lr, loss=np.array(hist), train_seconds=train_s)
+    log(f"saved {args.out} ({net.param_count} parameters, {train_s:.1f}s of training)")
+    del xs, ys
+    return net
+
+
+def load(path=WEIGHTS, max_batch=1):
+    d = np.load(path)
+    net = learn.UNet(tuple(int(v) for v in d["grid"]), max_batch=max_batch, seed=0)
+    net.set_params(d["params"])
+    return net
+
+
+class LearnedPath:
+    """Sparse beamforming + restoration + gate + fallback, with per-stage CUDA-event timing."""
+
+    def __init__(self, net):
+        self.net = net
+        self.sparse = Acquisition(SPARSE_T, GROUP)
+        self.full = Acquisition(FULL_T, 1)
+        self.gate_plan = Plan(acquisition_params(FULL_T, 1, sub=SUB))
+        Z, Y, X = GRID
+        self.vs = torch.empty((1, Z, Y, X), dtype=torch.complex64, device="cuda")
+        self.vo = torch.empty_like(self.vs)
+        self.vf = torch.empty((Z, Y, X), dtype=torch.complex64, device="cuda")
+        self.vg = torch.empty((Z // SUB, Y // SUB, X // SUB), dtype=torch.complex64, device="cuda")
+
+    def run(self, scat, seed):
+        """Acquires both schemes (untimed), then times the learned path and the plain path on
+        the device. Returns a dict of stage times (ms) and NRMSEs."""
+        self.sparse.acquire(scat, 2 * seed + 1)
+        self.full.acquire(scat, 2 * seed)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+        ev[0].record()
+        self.sparse.volume(out=self.vs[0])
+        ev[1].record()
+        self.net.forward(self.vs, out=self.vo)
+        ev[2].record()
+        # gate: full-transmit front end + sub-grid delay-and-sum, compared on the device
+        self.gate_plan.beamform(self.full.raw, out=self.vg)
+        self.vg /= self.full.gain
+        sub = self.vo[0, ::SUB, ::SUB, ::SUB]
+        est = torch.linalg.vector_norm(sub - self.vg) / torch.linalg.vector_norm(self.vg)
+        ev[3].record()
+        # plain full-transmit path (also the fallback)
+        self.full.volume(out=self.vf)
+        ev[4].record()
+        torch.cuda.synchronize()
+        t = [ev[i].elapsed_time(ev[i + 1]) for i in range(4)]
+        return dict(sparse_ms=t[0], unet_ms=t[1], gate_ms=t[2], full_ms=t[3], gate_nrmse=float(est),
+                    nrmse_net=nrmse(self.vo[0], self.vf), nrmse_plain=nrmse(self.vs[0], self.vf))
+
+
+def summarize(rows, bar=NRMSE_BAR):
+    """Volumes/s of the plain path and of the learned path with gate + fallback charged."""
+    n = len(rows)
+    full = sum(r["full_ms"] for r in rows)
+    passed = [r["gate_nrmse"] <= bar for r in rows]
+    learned = sum(r["sparse_ms"] + r["unet_ms"] + r["gate_ms"] + (0.0 if ok else r["full_ms"])
+                  for r, ok in zip(rows, passed))
+    true_ok = [r["nrmse_net"] <= bar for r in rows]
+    oracle_gated = sum(r["sparse_ms"] + r["unet_ms"] + (0.0 if ok else r["full_ms"]) for r, ok in zip(rows, true_ok))
+    delivered = [r["nrmse_net"] if ok else 0.0 for r, ok in zip(rows, passed)]
+    return dict(
+        volumes=n, plain_volumes_per_s=1e3 * n / full, learned_volumes_per_s=1e3 * n / learned,
+        learned_oracle_gated_volumes_per_s=1e3 * n / oracle_gated, speedup=full / learned,
+        gate_pass_fraction=sum(passed) / n, true_pass_fraction=sum(true_ok) / n,
+        nrmse_net_median=float(np.median([r["nrmse_net"] for r in rows])),
+        nrmse_net_mean=float(np.mean([r["nrmse_net"] for r in rows])),
+        nrmse_plain_sparse_median=float(np.median([r["nrmse_plain"] for r in rows])),
+        nrmse_delivered_max=float(max(delivered)) if delivered else 0.0,
+        gate_error_median=float(np.median([abs(r["gate_nrmse"] - r["nrmse_net"]) for r in rows])),
+        ms=dict(sparse=float(np.mean([r["sparse_ms"] for r in rows])), unet=float(np.mean([r["unet_ms"] for r in rows])),
+                gate=float(np.mean([r["gate_ms"] for r in rows])), full=float(np.mean([r["full_ms"] for r in rows]))))
+
+
+def evaluate(net, n, seed0=EVAL_SEED0, warmup=2, log=print):
+    path = LearnedPath(net)
+    for k in range(warmup):
+        path.run(torch.from_numpy(phantom(seed0 + k)).cuda(), seed0 + k)
+    rows = []
+    for k in range(n):
+        rows.append(path.run(torch.from_numpy(phantom(seed0 + k)).cuda(), seed0 + k))
+    path.full.plan.check()
+    path.sparse.plan.check()
+    net.check()
+    return summarize(rows), rows
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train")
+    t.add_argument("--phantoms", type=int, default=2048)
+    t.add_argument("--epochs", type=int, default=4)
+    t.add_argument("--batch", type=int, default=2)
+    t.add_argument("--lr", type=float, default=1e-3)
+    t.add_argument("--seed", type=int, default=1)
+    t.add_argument("--out", default=WEIGHTS)
+    t.add_argument("--eval", type=int, default=0, help="evaluate on this many held-out phantoms afterwards")
+    e = sub.add_parser("evaluate")
+    e.add_argument("--weights", default=WEIGHTS)
+    e.add_argument("--phantoms", type=int, default=256)
+    e.add_argument("--json", default=None)
+    a = ap.parse_args()
+    if a.cmd == "train":
+        net = train(a)
+        if a.eval:
+            s, _ = evaluate(net, a.eval)
+            print(json.dumps(s))
+    else:
+        net = load(a.weights)
+        s, rows = evaluate(net, a.phantoms)
+        print(json.dumps(s))
+        if a.json:
+            with open(a.json, "w") as f:
+                json.dump(dict(summary=s, rows=rows), f)
+
+
+if __name__ == "__main__":
+    main()

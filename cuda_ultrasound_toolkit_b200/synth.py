@@ -191,3 +191,17 @@ def frame(name: str, seed: int = None, data_type=InputDataTypes.TYPE_I16, channe
     if data_type == InputDataTypes.TYPE_F32:
         raw = raw.astype(np.float32)
     return raw, bp
+
+
+def phantom(rng, n_points, n_speckle=0, speckle_sigma=0.05, box_xy=9e-3, z_range=(10e-3, 40e-3)):
+    """Scatterers as float32 [n][4] (x, y, z, amplitude): n_points point targets with U(0.5, 1)
+    amplitudes plus n_speckle weak scatterers with N(0, speckle_sigma) amplitudes, all uniform
+    in the box."""
+    n = n_points + n_speckle
+    out = np.empty((n, 4), dtype=np.float32)
+    out[:, 0] = rng.uniform(-box_xy, box_xy, n)
+    out[:, 1] = rng.uniform(-box_xy, box_xy, n)
+    out[:, 2] = rng.uniform(z_range[0], z_range[1], n)
+    out[:n_points, 3] = rng.uniform(0.5, 1.0, n_points)
+    out[n_points:, 3] = rng.normal(0.0, speckle_sigma, n_speckle)
+    return out

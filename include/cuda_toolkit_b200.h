@@ -61,7 +61,7 @@ CUTB_API bool cutb_encoding_matrix(uint n, int ordering, signed char* out);
 /* Options that the parameter struct has no field for. Zero-initialise for defaults. */
 typedef struct cutb_options {
     int iq_bf16;      /* 1: analytic signal stored as bf16 complex (halves DAS gather bytes) */
-    int das_tile;     /* 0: tuned/default tile; >0: explicit tile id (autotuner) */
+    int das_tile;     /* delay-and-sum tile: 0 = chosen from the grid, 1 = 4x8x32, 2 = 8x8x16 (HERCULES) */
     int reserved[14];
 } cutb_options;
 

@@ -209,6 +209,24 @@ def test_das_vs_fp64(torch, orc, case):
         assert (got == got[:, :1, :]).all()
 
 
+TILE_CASES = [dict(), dict(cf=1.0, cubic=False), dict(focus_z=15e-3), dict(X=33, Y=3, Z=70),
+              dict(z=(10e-3, 14e-3)), dict(z=(10e-3, 13e-3), cf=1.0, fn_rx=1.5),
+              # staged windows with linear interpolation over many stages (C = 64 -> 8 per transmit)
+              dict(z=(10e-3, 14e-3), cubic=False, C=64, T=16), dict(z=(10e-3, 14e-3), cubic=False, cf=0.7, C=32)]
+
+
+@pytest.mark.parametrize("tile", [1, 2], ids=["tile4x8x32", "tile8x8x16"])
+@pytest.mark.parametrize("case", TILE_CASES, ids=lambda c: ",".join(f"{k}={v}" for k, v in c.items()) or "default")
+def test_das_tile_shapes(torch, orc, case, tile):
+    """Both HERCULES tile shapes (staged and direct windows) against the FP64 oracle."""
+    bp = das_params(**case)
+    S, C, T = bp.dims
+    iq = analytic_rows(orc, T, C, S, seed=3 + len(str(case)))
+    got = Plan(bp, das_tile=tile).das(torch.from_numpy(iq.astype(np.complex64)).cuda()).cpu().numpy()
+    tol = TOL_DAS_APO if "fn_rx" in case else TOL_DAS_RANDOM
+    assert rel_l2(got, orc.das(iq, bp)) < tol
+
+
 def test_das_bf16_storage(torch, orc):
     bp = das_params(cf=1.0)
     S, C, T = bp.dims

@@ -123,3 +123,38 @@ def test_das_is_linear(orc):
     vox = rng.integers(0, w.X * w.Y * w.Z, 16)
     np.testing.assert_allclose(orc.das(a + 2 * b, bp, vox), orc.das(a, bp, vox) + 2 * orc.das(b, bp, vox),
                                rtol=1e-10, atol=1e-9)
+
+
+def test_philox_known_answers():
+    """Philox4x32-10 known-answer vectors published with Random123 (Salmon et al., SC 2011)."""
+    from oracle import sim_ref
+    cases = [
+        ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+        ((0xFFFFFFFF,) * 4, (0xFFFFFFFF, 0xFFFFFFFF), (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+        ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+         (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)),
+    ]
+    for ctr, key, want in cases:
+        got = sim_ref.philox4x32_10(*[np.array([c], dtype=np.uint64) for c in ctr], *key)
+        assert tuple(int(g[0]) for g in got) == want
+
+
+def test_sim_ref_matches_numpy_generator():
+    """The simulator restatement without noise/encoding equals synth.echoes (one row per transmit)."""
+    from oracle import sim_ref
+    from cuda_ultrasound_toolkit_b200 import synth
+    w = synth.Workload("t", 8, 6, 512, 4, 4, 4, 7, cubic=True, cf=0.0, box_xy=2e-3, z_range=(3e-3, 6e-3))
+    pos, amp = synth.scatterer_field(w, np.random.default_rng(3))
+    scat = np.concatenate([pos, amp[:, None]], axis=1)
+    got = sim_ref.echoes(scat, 8, 1, 6, 512, synth.PITCH, synth.FS, synth.FC, synth.C_SOUND)
+    ref = synth.echoes(w, pos, amp)
+    assert np.max(np.abs(got - ref)) < 1e-5 * np.max(np.abs(ref))
+    # grouped rows: the sum over the group's rows
+    g4 = sim_ref.echoes(scat, 2, 4, 6, 512, synth.PITCH, synth.FS, synth.FC, synth.C_SOUND)
+    assert np.allclose(g4[0], got[0:4].sum(0)) and np.allclose(g4[1], got[4:8].sum(0))
+
+
+def test_sim_noise_is_standard_normal():
+    from oracle import sim_ref
+    z = sim_ref.gaussian_noise(200000, 77)
+    assert abs(z.mean()) < 0.01 and abs(z.std() - 1) < 0.01
