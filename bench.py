@@ -310,6 +310,8 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": launches,
         "clocks": clock,
     }
+    if args.learned > 0 and world == 1:
+        line["learned"] = learned_path(args.learned)
     try:
         per_vol, sample = cpu_sample(frames[0][0], bp, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": 1.0 / per_vol, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
@@ -320,12 +322,37 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def learned_path(volumes):
+    """The learned sparse-transmit path against the plain full-transmit path on held-out phantoms
+    (128 x 128 rows/columns, 4096 samples, 128^3 volume, cubic, no coherence factor): 32 transmits
+    on every 4th row -> delay-and-sum -> U-Net, gated by a full-transmit spot check (1/64 of the
+    tiles) with fallback to the full delay-and-sum above 2 % NRMSE; both paths timed on the device
+    from the int16 raw frames in HBM."""
+    from cuda_ultrasound_toolkit_b200 import sparse
+    if not os.path.exists(sparse.WEIGHTS):
+        return {"unavailable": f"no trained weights at {os.path.relpath(sparse.WEIGHTS, ROOT)}"}
+    try:
+        meta = np.load(sparse.WEIGHTS)
+        net = sparse.load(sparse.WEIGHTS)
+        summary, _ = sparse.evaluate(net, volumes)
+        summary.update({"nrmse_bar": sparse.NRMSE_BAR, "eval_seeds": f"{sparse.EVAL_SEED0}..",
+                        "network_parameters": net.param_count, "trained_phantoms": int(meta["phantoms"]),
+                        "trained_epochs": int(meta["epochs"]),
+                        "workload": "rca128 full 128-tx vs sparse 32-tx (every 4th row), 128^3, cubic, no CF"})
+        net.close()
+        return summary
+    except Exception as exc:  # the learned path must not hide the plain pipeline's number
+        return {"failed": str(exc)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--learned", type=int, default=16,
+                    help="held-out volumes for the learned sparse-transmit path (0: skip)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

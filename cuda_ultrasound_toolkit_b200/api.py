@@ -66,6 +66,8 @@ def lib():
         "cutb_debug_fail_allocations_after": ([ctypes.c_int], None),
         "cutb_calibrate_fp32": ([ctypes.POINTER(ctypes.c_double), vp], b),
         "cutb_plan_check": ([vp, vp], b),
+        "cutb_plan_das_tile_shape": ([vp, ctypes.POINTER(u)], b),
+        "cutb_das_tiles": ([vp, vp, vp, ctypes.POINTER(ctypes.c_int), u, u, vp], b),
         "init_cuda_configuration": ([ctypes.POINTER(u), ctypes.POINTER(u)], b),
         "register_cuda_buffers": ([ctypes.POINTER(u), u, u], b),
         "cuda_set_channel_mapping": ([ctypes.POINTER(ctypes.c_int16)], b),
@@ -224,6 +226,21 @@ class Plan:
     def das(self, iq, out=None, stream=None):
         out = self.empty_volume() if out is None else out
         _check(lib().cutb_das(self._h, iq.data_ptr(), out.data_ptr(), _stream_handle(stream)), "cutb_das")
+        return out
+
+    @property
+    def tile_shape(self):
+        """(x, y, z) voxels of a delay-and-sum tile."""
+        shape = (ctypes.c_uint * 3)()
+        _check(lib().cutb_plan_das_tile_shape(self._h, shape), "cutb_plan_das_tile_shape")
+        return tuple(shape)
+
+    def das_tiles(self, iq, tiles, splits=1, out=None, stream=None):
+        """Delay-and-sum of the listed tile ids only (others zero), stages split over `splits` CTAs."""
+        out = self.empty_volume() if out is None else out
+        t = np.ascontiguousarray(tiles, dtype=np.int32)
+        _check(lib().cutb_das_tiles(self._h, iq.data_ptr(), out.data_ptr(), t.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                    t.size, splits, _stream_handle(stream)), "cutb_das_tiles")
         return out
 
     def check(self, stream=None):

@@ -474,7 +474,19 @@ das_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
     // ---- tile, voxels, offsets from the tile centre -----------------------------------------
-    const int tx0 = blockIdx.x * L::TX, ty0 = blockIdx.y * L::TY, tz0 = blockIdx.z * L::TZ;
+    // Whole grid: blockIdx.xyz is the tile. Tile list: blockIdx.x indexes a.tiles and
+    // blockIdx.y is the slice of the stages (transmits x channel groups) this CTA sums.
+    int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
+    int split = 0;
+    if (a.tiles) {
+        const int nx = div_up(a.X, L::TX), ny = div_up(a.Y, L::TY);
+        const int id = a.tiles[blockIdx.x];
+        bx = id % nx;
+        by = (id / nx) % ny;
+        bz = id / (nx * ny);
+        split = blockIdx.y;
+    }
+    const int tx0 = bx * L::TX, ty0 = by * L::TY, tz0 = bz * L::TZ;
     const float ix_c = tx0 + 0.5f * (L::TX - 1), iy_c = ty0 + 0.5f * (L::TY - 1), iz_c = tz0 + 0.5f * (L::TZ - 1);
     Tile tile;
     tile.cx = (double)a.vmin_x + (double)ix_c * (double)a.res_x;
@@ -544,24 +556,29 @@ das_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
     }
 
     const int nchunks = div_up(a.C, kRows);
-    const int nstages = a.T * nchunks * a.G;
+    const int total_stages = a.T * nchunks * a.G;
+    // This CTA's stages: all of them, or slice `split` of a.splits.
+    const int k_begin = a.splits > 1 ? (int)((long long)total_stages * split / a.splits) : 0;
+    const int nstages = a.splits > 1 ? (int)((long long)total_stages * (split + 1) / a.splits) : total_stages;
     // Window metadata (FP64) is computed for kBatch stages at a time by all threads; a stage's
     // bulk copies are then issued by lanes 0..kRows-1 of warp 0, one row per lane.
     static_assert(kRows <= 32 && kStages <= kBatch, "issue layout");
-    compute_batch<SEQ>(sm, 0, nstages, nchunks, a, tile);
+    compute_batch<SEQ>(sm, k_begin, nstages, nchunks, a, tile);
     __syncthreads();
     if (warp == 0 && lane < kRows)
-        for (int k = 0; k < kStages && k < nstages; ++k) issue_row(sm, k, k, lane, a, iq);
+        for (int j = 0; j < kStages && k_begin + j < nstages; ++j) issue_row(sm, j, k_begin + j, lane, a, iq);
 
-    for (int k = 0; k < nstages; ++k) {
-        const int b = k % kStages;
-        if (!mbar_wait_bounded(&sm.full[b], (unsigned)(k / kStages) & 1u)) {
+    for (int k = k_begin; k < nstages; ++k) {
+        const int j = k - k_begin;  // local stage number: buffer and barrier phase
+        const int b = j % kStages;
+        if (!mbar_wait_bounded(&sm.full[b], (unsigned)(j / kStages) & 1u)) {
             sm.abort = 1;
             atomicOr(a.status, 1);
         }
         const StageMeta st = sm.stage[b];
         const int next = k + kStages;  // stage that refills buffer b
-        if (next < nstages && next % kBatch == 0) compute_batch<SEQ>(sm, next, nstages, nchunks, a, tile);
+        if (next < nstages && (next - k_begin) % kBatch == 0)
+            compute_batch<SEQ>(sm, next, nstages, nchunks, a, tile);
         int all_staged = 1;
         if constexpr (CUBIC) {
             build_coefficients(sm, b, st.nq);
@@ -624,7 +641,11 @@ das_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
             out.x *= cf;
             out.y *= cf;
         }
-        if (HERC) {
+        if (a.splits > 1) {  // partial sums over a slice of the stages (no coherence factor)
+            float2* o = vol + ((size_t)z * a.Y + y_idx) * a.X + x_idx;
+            atomicAdd(&o->x, out.x);
+            atomicAdd(&o->y, out.y);
+        } else if (HERC) {
             vol[((size_t)z * a.Y + y_idx) * a.X + x_idx] = out;
         } else {
             for (int y = 0; y < a.Y; ++y) vol[((size_t)z * a.Y + y) * a.X + x_idx] = out;
@@ -636,7 +657,8 @@ template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT>
 bool launch_das_t(const DasArgs& a, const void* iq, void* volume, cudaStream_t st)
 {
     using L = Layout<SEQ, SHORT>;
-    const dim3 grid(div_up(a.X, L::TX), div_up(a.Y, L::TY), div_up(a.Z, L::TZ));
+    dim3 grid(div_up(a.X, L::TX), div_up(a.Y, L::TY), div_up(a.Z, L::TZ));
+    if (a.tiles) grid = dim3(a.ntiles, a.splits > 1 ? a.splits : 1, 1);
     CUTB_REQUIRE(grid.y <= 65535 && grid.z <= 65535, CUTB_ERR_UNSUPPORTED, "Output grid too large.");
     auto kern = das_kernel<SEQ, CUBIC, CF, APO, IQ, SHORT>;
     const size_t smem = sizeof(Smem<IQ, CUBIC>);
@@ -780,6 +802,19 @@ bool derive_das(const CudaBeamformerParameters& bp, DasArgs& a)
     return true;
 }
 
+static bool use_short_tile(const DasArgs& a)
+{
+    return a.seq == HERCULES && (a.tile == 2 || (a.tile == 0 && prefer_short_tile(a)));
+}
+
+void das_tile_shape(const DasArgs& a, int shape[3])
+{
+    const bool sh = use_short_tile(a);
+    shape[0] = a.seq == HERCULES ? (sh ? Layout<HERCULES, true>::TX : Layout<HERCULES, false>::TX) : Layout<FORCES, false>::TX;
+    shape[1] = a.seq == HERCULES ? 8 : 1;
+    shape[2] = sh ? Layout<HERCULES, true>::TZ : Layout<HERCULES, false>::TZ;
+}
+
 bool launch_das(const DasArgs& a, const void* iq, bool iq_bf16, void* volume, cudaStream_t st, int* launches)
 {
     CUTB_REQUIRE(a.status != nullptr, CUTB_ERR_NOT_INITIALIZED, "Delay-and-sum status word not allocated.");
@@ -788,7 +823,10 @@ bool launch_das(const DasArgs& a, const void* iq, bool iq_bf16, void* volume, cu
     CUTB_REQUIRE(a.S % 4 == 0, CUTB_ERR_UNSUPPORTED,
                  "Delay-and-sum needs a sample count that is a multiple of 4 (got %d).", a.S);
     bool ok;
-    if (a.seq == HERCULES && (a.tile == 2 || (a.tile == 0 && prefer_short_tile(a))))
+    CUTB_REQUIRE(!a.tiles || (a.ntiles > 0 && a.ntiles <= (1 << 24)), CUTB_ERR_INVALID_ARGUMENT, "Bad tile list.");
+    CUTB_REQUIRE(a.splits <= 1 || (a.tiles && !a.apply_cf && a.seq == HERCULES), CUTB_ERR_UNSUPPORTED,
+                 "Split delay-and-sum needs a tile list, HERCULES and no coherence factor.");
+    if (use_short_tile(a))
         ok = iq_bf16 ? launch_das_s<HERCULES, __nv_bfloat162, true>(a, iq, volume, st)
                      : launch_das_s<HERCULES, float2, true>(a, iq, volume, st);
     else if (a.seq == HERCULES)

@@ -285,6 +285,49 @@ CUTB_API bool cutb_das(cutb_plan* p, const void* d_iq, void* d_volume, void* str
     return launch_das(p->das, d_iq, p->iq_bf16, d_volume, (cudaStream_t)stream, &p->launches);
 }
 
+CUTB_API bool cutb_plan_das_tile_shape(const cutb_plan* p, uint shape[3])
+{
+    CUTB_REQUIRE(p && shape, CUTB_ERR_INVALID_ARGUMENT, "Null argument.");
+    int s[3];
+    das_tile_shape(p->das, s);
+    for (int i = 0; i < 3; ++i) shape[i] = (uint)s[i];
+    return true;
+}
+
+CUTB_API bool cutb_das_tiles(cutb_plan* p, const void* d_iq, void* d_volume, const int* tiles, uint ntiles,
+                             uint splits, void* stream)
+{
+    CUTB_REQUIRE(p, CUTB_ERR_INVALID_ARGUMENT, "Null plan.");
+    CUTB_REQUIRE(d_iq && d_volume && tiles && ntiles > 0, CUTB_ERR_INVALID_ARGUMENT, "Null or empty argument.");
+    CUTB_REQUIRE(p->das.seq == HERCULES && !p->das.apply_cf, CUTB_ERR_UNSUPPORTED,
+                 "Tile-list delay-and-sum supports HERCULES without coherence factor.");
+    CUTB_REQUIRE(splits >= 1 && splits <= 4096 && ntiles <= (1u << 24), CUTB_ERR_INVALID_ARGUMENT,
+                 "splits must be 1..4096.");
+    int shape[3];
+    das_tile_shape(p->das, shape);
+    const long long total = (long long)div_up(p->das.X, shape[0]) * div_up(p->das.Y, shape[1]) *
+                            div_up(p->das.Z, shape[2]);
+    for (uint i = 0; i < ntiles; ++i)
+        CUTB_REQUIRE(tiles[i] >= 0 && tiles[i] < total, CUTB_ERR_INVALID_ARGUMENT, "Tile id %d outside 0..%lld.",
+                     tiles[i], total - 1);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (ntiles > p->tiles_capacity) {
+        device_free(p->d_tiles);
+        p->d_tiles = nullptr;
+        p->tiles_capacity = 0;
+        if (!alloc_bytes((void**)&p->d_tiles, sizeof(int) * ntiles)) return false;
+        p->tiles_capacity = ntiles;
+    }
+    CUTB_CUDA_OK(cudaMemcpyAsync(p->d_tiles, tiles, sizeof(int) * ntiles, cudaMemcpyHostToDevice, st));
+    CUTB_CUDA_OK(cudaMemsetAsync(d_volume, 0, p->vol_bytes, st));
+    DasArgs a = p->das;
+    a.tiles = p->d_tiles;
+    a.ntiles = (int)ntiles;
+    a.splits = (int)splits;
+    p->launches = 0;
+    return launch_das(a, d_iq, p->iq_bf16, d_volume, st, &p->launches);
+}
+
 CUTB_API bool cutb_plan_check(cutb_plan* p, void* stream)
 {
     CUTB_REQUIRE(p, CUTB_ERR_INVALID_ARGUMENT, "Null plan.");
@@ -359,4 +402,5 @@ cutb_plan::~cutb_plan()
     device_free(d_decoded);
     device_free(d_iq);
     device_free(d_status);
+    device_free(d_tiles);
 }

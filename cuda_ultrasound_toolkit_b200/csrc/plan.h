@@ -45,6 +45,8 @@ struct cutb_plan {
     float* d_decoded = nullptr;
     void* d_iq = nullptr;
     int* d_status = nullptr;   // device-side error word of the stage kernels
+    int* d_tiles = nullptr;    // tile list of cutb_das_tiles
+    uint32_t tiles_capacity = 0;
     int launches = 0;
 
     bool build(const CudaBeamformerParameters& params, const cutb_options* options);

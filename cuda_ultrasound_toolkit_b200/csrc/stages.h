@@ -70,6 +70,9 @@ struct DasArgs {
     float to_power;            // sine apodization exponent
     unsigned long long readi_row;  // bit g set: sub-signal g negated
     int tile;                  // HERCULES tile: 0 chosen from the grid, 1 = 4 x 8 x 32, 2 = 8 x 8 x 16
+    const int* tiles;          // optional device list of tile ids (z-major); null = every tile
+    int ntiles;
+    int splits;                // > 1: stages split across CTAs, partial sums added atomically
     int* status;               // device word: bit 0 set when a bounded wait gave up
 };
 
@@ -77,5 +80,7 @@ struct DasArgs {
 // validation as the upstream dispatcher (beamformer.cu:17-197).
 bool derive_das(const CudaBeamformerParameters& bp, DasArgs& a);
 bool launch_das(const DasArgs& a, const void* iq, bool iq_bf16, void* volume, cudaStream_t st, int* launches);
+// Tile shape (x, y, z voxels) the delay-and-sum kernel uses for these arguments.
+void das_tile_shape(const DasArgs& a, int shape[3]);
 
 }  // namespace cutb

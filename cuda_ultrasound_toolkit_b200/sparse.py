@@ -3,10 +3,11 @@ the U-Net (csrc/unet.cu, trained by the library's own tcgen05 kernels), and gate
 with an online NRMSE estimate against the plain full-transmit delay-and-sum, falling back to
 the full-transmit volume when the estimate exceeds the bar.
 
-Acquisitions (row-column array, 128 receive columns, 4096 samples, fs 20 MHz, pitch 0.3 mm):
+Acquisitions (row-column array of 128 transmit rows and 128 receive columns, 4096 samples,
+fs 20 MHz, pitch 0.3 mm):
   full    128 transmit events, one row each, order-128 Hadamard encoding
-  sparse   32 transmit events, 4 adjacent rows fired together (a 1.2 mm virtual element),
-           order-32 Hadamard encoding
+  sparse   32 transmit events on every 4th row (rows 2, 6, ..., 126), order-32 Hadamard
+           encoding -- a 4x sparser transmit aperture of the same extent
 Both are beamformed by the plain pipeline (decode + Hilbert + delay-and-sum, cubic
 interpolation, no coherence factor) onto the same 128^3 grid over x, y in [-9, 9] mm and
 z in [10, 40] mm, and divided by the simulator's gain, so volumes are in scatterer units.
@@ -15,9 +16,11 @@ Phantoms: 50-400 point scatterers with U(0.5, 1) amplitudes plus 20 000 speckle 
 with N(0, 0.05) amplitudes, uniform in the box; phantom k is seeded by k.
 
 NRMSE = ||V_hat - V|| / ||V|| over the complex volume, V the plain full-transmit volume.
-Gate: the full-transmit delay-and-sum on the 32^3 sub-grid of every 4th voxel (1/64 of the
-voxels) estimates the NRMSE of the restored volume; above 2 % the volume falls back to the
-full-transmit delay-and-sum, whose cost is charged to the learned path.
+Gate: the full-transmit front end runs, and the full-transmit delay-and-sum is evaluated on a
+fixed, seeded 1/64 of the delay-and-sum tiles (cutb_das_tiles, stages split over CTAs); its
+NRMSE against the restored volume on those voxels is the estimate. Above 2 % the volume falls
+back to the full-transmit delay-and-sum of the already decoded analytic signal, whose cost is
+charged to the learned path.
 
   python -m cuda_ultrasound_toolkit_b200.sparse train --phantoms 2048 --epochs 4 --out weights.npz
   python -m cuda_ultrasound_toolkit_b200.sparse evaluate --weights weights.npz --phantoms 256
@@ -36,31 +39,31 @@ from .api import Plan
 from .simulate import Simulator
 
 C, S = 128, 4096
-FULL_T, SPARSE_T, GROUP = 128, 32, 4
+ROWS = 128                        # transmit rows of the array
+FULL_T, SPARSE_T = 128, 32
+SPARSE_STRIDE, SPARSE_OFFSET = 4, 2
 GRID = (128, 128, 128)            # Z, Y, X
 BOX_XY, Z_RANGE = 9e-3, (10e-3, 40e-3)
 N_SPECKLE = 20000
 NRMSE_BAR = 0.02
-SUB = 4                           # gate sub-grid stride
+GATE_FRACTION = 64                # the gate evaluates 1 in GATE_FRACTION tiles
+GATE_SPLITS = 16                  # stage slices per gate tile
 TRAIN_SEED0, EVAL_SEED0 = 0, 1_000_000
 CHANNEL_MAP = np.arange(C, dtype=np.int16)
 WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "unet_sparse4.npz")
 
 
-def acquisition_params(T, G, grid=GRID, sub=1):
-    """Pipeline parameters for T transmit events of G rows; sub > 1 gives the gate's sub-grid."""
+def acquisition_params(T, stride=1, offset=0, grid=GRID):
+    """Pipeline parameters for T transmit events on rows offset, offset + stride, ... of the array."""
     Z, Y, X = grid
-    w = synth.Workload("sparse" if G > 1 else "full", T, C, S, X // sub, Y // sub, Z // sub, 0, cubic=True, cf=0.0,
+    w = synth.Workload("full" if stride == 1 else "sparse", T, C, S, X, Y, Z, 0, cubic=True, cf=0.0,
                        box_xy=BOX_XY, z_range=Z_RANGE)
     bp = synth.make_params(w, channel_map=CHANNEL_MAP)
-    bp.xdc_element_pitch[1] = G * synth.PITCH
-    bp.xdc_transform[13] = T * G * synth.PITCH / 2
-    if sub > 1:
-        rx = 2 * BOX_XY / (X - 1)
-        rz = (Z_RANGE[1] - Z_RANGE[0]) / (Z - 1)
-        bp.output_max_coordinate[0] = -BOX_XY + (X - sub) * rx
-        bp.output_max_coordinate[1] = -BOX_XY + (Y - sub) * rx
-        bp.output_max_coordinate[2] = Z_RANGE[0] + (Z - sub) * rz
+    # Transmit j sits on row r = offset + j * stride at y = -ROWS p / 2 + p / 2 + r p; the
+    # beamformer places it at -xdc_transform[13] + pitch_y / 2 + j * pitch_y.
+    p = synth.PITCH
+    bp.xdc_element_pitch[1] = stride * p
+    bp.xdc_transform[13] = ROWS * p / 2 - offset * p + (stride - 1) * p / 2
     return bp
 
 
@@ -72,9 +75,9 @@ def phantom(seed):
 class Acquisition:
     """Simulator + pipeline for one transmit scheme; volumes in scatterer units."""
 
-    def __init__(self, T, G, sub=1):
-        self.sim = Simulator(T, C, S, rows_per_transmit=G)
-        self.plan = Plan(acquisition_params(T, G, sub=sub))
+    def __init__(self, T, stride=1, offset=0):
+        self.sim = Simulator(T, C, S, row_stride=stride, row_offset=offset, array_rows=ROWS)
+        self.plan = Plan(acquisition_params(T, stride, offset))
         self.raw = torch.empty((C, T * S), dtype=torch.int16, device="cuda")
         self.gain = torch.empty(1, dtype=torch.float32, device="cuda")
 
@@ -88,6 +91,14 @@ class Acquisition:
         return out
 
 
+def full_acquisition():
+    return Acquisition(FULL_T)
+
+
+def sparse_acquisition():
+    return Acquisition(SPARSE_T, SPARSE_STRIDE, SPARSE_OFFSET)
+
+
 def nrmse(est, ref):
     return float(torch.linalg.vector_norm(est - ref) / torch.linalg.vector_norm(ref))
 
@@ -97,7 +108,7 @@ def make_pairs(n, seed0, log=print):
     Z, Y, X = GRID
     xs = torch.empty((n, Z, Y, X), dtype=torch.complex64, device="cuda")
     ys = torch.empty_like(xs)
-    full, sparse = Acquisition(FULL_T, 1), Acquisition(SPARSE_T, GROUP)
+    full, sparse = full_acquisition(), sparse_acquisition()
     t0 = time.time()
     for k in range(n):
         scat = torch.from_numpy(phantom(seed0 + k)).cuda()
@@ -153,62 +164,79 @@ class LearnedPath:
 
     def __init__(self, net):
         self.net = net
-        self.sparse = Acquisition(SPARSE_T, GROUP)
-        self.full = Acquisition(FULL_T, 1)
-        self.gate_plan = Plan(acquisition_params(FULL_T, 1, sub=SUB))
+        self.sparse = sparse_acquisition()
+        self.full = full_acquisition()
         Z, Y, X = GRID
         self.vs = torch.empty((1, Z, Y, X), dtype=torch.complex64, device="cuda")
         self.vo = torch.empty_like(self.vs)
         self.vf = torch.empty((Z, Y, X), dtype=torch.complex64, device="cuda")
-        self.vg = torch.empty((Z // SUB, Y // SUB, X // SUB), dtype=torch.complex64, device="cuda")
+        self.vg = torch.empty_like(self.vf)
+        self.dec = self.full.plan.empty_decoded()
+        self.iq = self.full.plan.empty_iq()
+        tx, ty, tz = self.full.plan.tile_shape
+        nx, ny, nz = -(-X // tx), -(-Y // ty), -(-Z // tz)
+        n = nx * ny * nz
+        rng = np.random.default_rng(20260101)
+        self.gate_tiles = np.sort(rng.choice(n, max(1, n // GATE_FRACTION), replace=False)).astype(np.int32)
+        mask = torch.zeros((Z, Y, X), dtype=torch.bool)
+        for i in self.gate_tiles:
+            x, y, z = i % nx, (i // nx) % ny, i // (nx * ny)
+            mask[z * tz:(z + 1) * tz, y * ty:(y + 1) * ty, x * tx:(x + 1) * tx] = True
+        self.mask = mask.cuda()
 
     def run(self, scat, seed):
-        """Acquires both schemes (untimed), then times the learned path and the plain path on
-        the device. Returns a dict of stage times (ms) and NRMSEs."""
+        """Acquires both schemes (untimed), then times the learned path's stages and the plain
+        path on the device. Returns stage times (ms) and NRMSEs."""
         self.sparse.acquire(scat, 2 * seed + 1)
         self.full.acquire(scat, 2 * seed)
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+        plan = self.full.plan
         ev[0].record()
         self.sparse.volume(out=self.vs[0])
         ev[1].record()
         self.net.forward(self.vs, out=self.vo)
         ev[2].record()
-        # gate: full-transmit front end + sub-grid delay-and-sum, compared on the device
-        self.gate_plan.beamform(self.full.raw, out=self.vg)
-        self.vg /= self.full.gain
-        sub = self.vo[0, ::SUB, ::SUB, ::SUB]
-        est = torch.linalg.vector_norm(sub - self.vg) / torch.linalg.vector_norm(self.vg)
+        plan.decode(self.full.raw, out=self.dec)
+        plan.hilbert(self.dec, out=self.iq)
         ev[3].record()
-        # plain full-transmit path (also the fallback)
-        self.full.volume(out=self.vf)
+        plan.das_tiles(self.iq, self.gate_tiles, splits=GATE_SPLITS, out=self.vg)
+        self.vg /= self.full.gain
+        g = self.vg[self.mask]
+        est = torch.linalg.vector_norm(self.vo[0][self.mask] - g) / torch.linalg.vector_norm(g)
         ev[4].record()
+        plan.das(self.iq, out=self.vf)   # plain path's delay-and-sum, also the fallback
+        self.vf /= self.full.gain
+        ev[5].record()
         torch.cuda.synchronize()
-        t = [ev[i].elapsed_time(ev[i + 1]) for i in range(4)]
-        return dict(sparse_ms=t[0], unet_ms=t[1], gate_ms=t[2], full_ms=t[3], gate_nrmse=float(est),
+        t = [ev[i].elapsed_time(ev[i + 1]) for i in range(5)]
+        return dict(sparse_ms=t[0], unet_ms=t[1], front_ms=t[2], gate_ms=t[3], das_ms=t[4], gate_nrmse=float(est),
                     nrmse_net=nrmse(self.vo[0], self.vf), nrmse_plain=nrmse(self.vs[0], self.vf))
 
 
 def summarize(rows, bar=NRMSE_BAR):
-    """Volumes/s of the plain path and of the learned path with gate + fallback charged."""
+    """Volumes/s of the plain path (front end + delay-and-sum of the full acquisition) and of
+    the learned path (sparse volume + network + full front end + gate, plus the full
+    delay-and-sum for every volume the gate rejects)."""
     n = len(rows)
-    full = sum(r["full_ms"] for r in rows)
+    plain = sum(r["front_ms"] + r["das_ms"] for r in rows)
     passed = [r["gate_nrmse"] <= bar for r in rows]
-    learned = sum(r["sparse_ms"] + r["unet_ms"] + r["gate_ms"] + (0.0 if ok else r["full_ms"])
+    learned = sum(r["sparse_ms"] + r["unet_ms"] + r["front_ms"] + r["gate_ms"] + (0.0 if ok else r["das_ms"])
                   for r, ok in zip(rows, passed))
     true_ok = [r["nrmse_net"] <= bar for r in rows]
-    oracle_gated = sum(r["sparse_ms"] + r["unet_ms"] + (0.0 if ok else r["full_ms"]) for r, ok in zip(rows, true_ok))
+    oracle_gated = sum(r["sparse_ms"] + r["unet_ms"] + (0.0 if ok else r["front_ms"] + r["das_ms"])
+                       for r, ok in zip(rows, true_ok))
     delivered = [r["nrmse_net"] if ok else 0.0 for r, ok in zip(rows, passed)]
+    mean = lambda k: float(np.mean([r[k] for r in rows]))  # noqa: E731
     return dict(
-        volumes=n, plain_volumes_per_s=1e3 * n / full, learned_volumes_per_s=1e3 * n / learned,
-        learned_oracle_gated_volumes_per_s=1e3 * n / oracle_gated, speedup=full / learned,
+        volumes=n, plain_volumes_per_s=1e3 * n / plain, learned_volumes_per_s=1e3 * n / learned,
+        learned_oracle_gated_volumes_per_s=1e3 * n / oracle_gated, speedup=plain / learned,
         gate_pass_fraction=sum(passed) / n, true_pass_fraction=sum(true_ok) / n,
-        nrmse_net_median=float(np.median([r["nrmse_net"] for r in rows])),
-        nrmse_net_mean=float(np.mean([r["nrmse_net"] for r in rows])),
+        nrmse_net_median=float(np.median([r["nrmse_net"] for r in rows])), nrmse_net_mean=mean("nrmse_net"),
         nrmse_plain_sparse_median=float(np.median([r["nrmse_plain"] for r in rows])),
         nrmse_delivered_max=float(max(delivered)) if delivered else 0.0,
         gate_error_median=float(np.median([abs(r["gate_nrmse"] - r["nrmse_net"]) for r in rows])),
-        ms=dict(sparse=float(np.mean([r["sparse_ms"] for r in rows])), unet=float(np.mean([r["unet_ms"] for r in rows])),
-                gate=float(np.mean([r["gate_ms"] for r in rows])), full=float(np.mean([r["full_ms"] for r in rows]))))
+        ms=dict(sparse=mean("sparse_ms"), unet=mean("unet_ms"), front=mean("front_ms"), gate=mean("gate_ms"),
+                das=mean("das_ms")))
 
 
 def evaluate(net, n, seed0=EVAL_SEED0, warmup=2, log=print):

@@ -94,6 +94,18 @@ CUTB_API bool cutb_das(cutb_plan* plan, const void* d_iq, void* d_volume, void* 
 /* Whole pipeline on device memory, intermediates in the plan's own buffers. */
 CUTB_API bool cutb_beamform(cutb_plan* plan, const void* d_raw, size_t raw_bytes, void* d_volume, void* stream);
 
+/* Tile shape (x, y, z voxels) of this plan's delay-and-sum; tile id = (tz * ny + ty) * nx + tx
+ * with nx = ceil(X / shape[0]) etc. */
+CUTB_API bool cutb_plan_das_tile_shape(const cutb_plan* plan, uint shape[3]);
+
+/* Delay-and-sum of the listed tiles only (host array of tile ids), each tile's transmit x channel
+ * stages split over `splits` CTAs whose partial sums are added atomically, so that a small set of
+ * tiles still fills the GPU. d_volume [Z][Y][X] is cleared first; voxels outside the listed tiles
+ * stay zero. HERCULES without coherence factor (the factor needs the complete sums). No
+ * counterpart upstream: it serves spot checks of a volume against the full delay-and-sum. */
+CUTB_API bool cutb_das_tiles(cutb_plan* plan, const void* d_iq, void* d_volume, const int* tiles, uint ntiles,
+                             uint splits, void* stream);
+
 /* Synchronises `stream` and reports whether a kernel of this plan hit a bounded device-side
  * wait (CUTB_ERR_TIMEOUT); clears the flag. cuda_toolkit::beamform calls it on every frame. */
 CUTB_API bool cutb_plan_check(cutb_plan* plan, void* stream);

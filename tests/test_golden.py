@@ -73,3 +73,17 @@ def test_golden_files_are_reproducible():
     v = _load("volumes.npz")
     bp = _params(v["hercules_readi_walsh.params"])
     assert np.array_equal(ref.beamform(v["raw"], bp), v["hercules_readi_walsh.volume"])
+
+
+def test_trained_weights_are_committed():
+    """The learned path's weights ship with the package and match the network's layout."""
+    import os
+    from cuda_ultrasound_toolkit_b200 import sparse
+    assert os.path.exists(sparse.WEIGHTS)
+    d = np.load(sparse.WEIGHTS)
+    assert tuple(d["grid"]) == sparse.GRID
+    # 11 layers: sum over layers of cout * (27 * cin + 1) in the padded master layout
+    specs = [(16, 16), (16, 16), (16, 32), (32, 32), (32, 64), (64, 64), (64, 64), (128, 32), (64, 16), (32, 16),
+             (16, 16)]
+    assert d["params"].size == sum(co * (27 * ci + 1) for ci, co in specs)
+    assert np.all(np.isfinite(d["params"]))

@@ -227,6 +227,37 @@ def test_das_tile_shapes(torch, orc, case, tile):
     assert rel_l2(got, orc.das(iq, bp)) < tol
 
 
+@pytest.mark.parametrize("splits", [1, 3, 16])
+@pytest.mark.parametrize("tile", [1, 2])
+def test_das_tile_list(torch, orc, splits, tile):
+    """Listed tiles with split stage slices equal the whole-grid delay-and-sum there; other voxels are 0."""
+    bp = das_params(z=(10e-3, 14e-3), C=24, T=8, X=24, Y=16, Z=64)
+    S, C, T = bp.dims
+    iq = torch.from_numpy(analytic_rows(orc, T, C, S, seed=4).astype(np.complex64)).cuda()
+    plan = Plan(bp, das_tile=tile)
+    full = plan.das(iq).cpu().numpy()
+    tx, ty, tz = plan.tile_shape
+    nx, ny, nz = -(-24 // tx), -(-16 // ty), -(-64 // tz)
+    ids = np.array(sorted(set([0, nx * ny * nz - 1, 5 % (nx * ny * nz), (nx * ny * nz) // 2])), dtype=np.int32)
+    got = plan.das_tiles(iq, ids, splits=splits).cpu().numpy()
+    mask = np.zeros(full.shape, bool)
+    for i in ids:
+        x, y, z = i % nx, (i // nx) % ny, i // (nx * ny)
+        mask[z * tz:(z + 1) * tz, y * ty:(y + 1) * ty, x * tx:(x + 1) * tx] = True
+    assert np.all(got[~mask] == 0)
+    assert rel_l2(got[mask], full[mask]) < 1e-6
+    plan.check()
+
+
+def test_das_tile_list_rejects_bad_ids(torch):
+    plan = Plan(das_params(z=(10e-3, 14e-3)))
+    iq = plan.empty_iq()
+    with pytest.raises(CutbError):
+        plan.das_tiles(iq, [-1])
+    with pytest.raises(CutbError):
+        plan.das_tiles(iq, [10 ** 6])
+
+
 def test_das_bf16_storage(torch, orc):
     bp = das_params(cf=1.0)
     S, C, T = bp.dims
