@@ -72,6 +72,72 @@ constexpr uint32_t tmem_cols_for(int cols)
     return cols <= 32 ? 32 : cols <= 64 ? 64 : cols <= 128 ? 128 : cols <= 256 ? 256 : 512;
 }
 
+// Epilogue of one output voxel (one TMEM lane): reads the COUT accumulator columns starting at
+// `col_addr` (a warp-collective tcgen05.ld per 8 columns, so every lane calls it) and applies the
+// requested epilogue; `valid` guards the memory accesses of voxels outside the volume.
+template <int COUT>
+__device__ __forceinline__ void conv_epilogue_voxel(const ConvFwdArgs& a, uint32_t col_addr, int n, size_t vox,
+                                                    bool valid, size_t plane, float& loss)
+{
+    if (a.epilogue == kEpiComplexOut || a.epilogue == kEpiLossGrad) {
+        float v[8];
+        tmem_ld8(col_addr, v);
+        tmem_wait_ld();
+        if (!valid) return;
+        const float f0 = v[0] + (a.bias ? a.bias[0] : 0.f), f1 = v[1] + (a.bias ? a.bias[1] : 0.f);
+        const size_t e = (size_t)n * plane + vox;
+        const float2 in = a.res[e];
+        const float s = a.scale[n];
+        if (a.epilogue == kEpiComplexOut) {
+            a.out_c[e] = make_float2(in.x + s * f0, in.y + s * f1);
+        } else {
+            const float2 tg = a.target[e];
+            const float inv = 1.f / s;
+            const float d0 = in.x * inv + f0 - tg.x * inv, d1 = in.y * inv + f1 - tg.y * inv;
+            loss += d0 * d0 + d1 * d1;
+            float g[8] = {a.grad_scale * d0, a.grad_scale * d1, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            uint4* o = reinterpret_cast<uint4*>(a.out) + ((size_t)n * a.out_cb_total + a.out_cb_offset) * plane + vox;
+            o[0] = pack_bf16x8(g);
+            for (int q = 1; q < COUT / 8; ++q) o[(size_t)q * plane] = make_uint4(0, 0, 0, 0);
+        }
+        return;
+    }
+#pragma unroll 1
+    for (int q = 0; q < COUT / 8; ++q) {
+        float v[8];
+        tmem_ld8(col_addr + q * 8, v);
+        tmem_wait_ld();
+        if (!valid) continue;
+        if (a.epilogue == kEpiMask) {
+            const uint4 m =
+                reinterpret_cast<const uint4*>(a.mask)[((size_t)n * a.mask_cb_total + a.mask_cb_offset + q) * plane + vox];
+            float mf[8];
+            unpack_bf16x8(m, mf);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = mf[i] > 0.f ? v[i] : 0.f;
+        } else {
+            if (a.bias) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) v[i] += __ldg(a.bias + q * 8 + i);
+            }
+            if (a.epilogue == kEpiBiasRelu) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) v[i] = fmaxf(v[i], 0.f);
+            }
+        }
+        reinterpret_cast<uint4*>(a.out)[((size_t)n * a.out_cb_total + a.out_cb_offset + q) * plane + vox] =
+            pack_bf16x8(v);
+    }
+}
+
+__device__ __forceinline__ void flush_loss(const ConvFwdArgs& a, float loss, int lane)
+{
+    if (a.epilogue != kEpiLossGrad) return;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
+    if (lane == 0) atomicAdd(a.loss, loss);
+}
+
 // ---- forward ---------------------------------------------------------------------------------
 template <int CB_IN, int COUT, int MT>
 struct FwdCfg {
@@ -187,63 +253,173 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(const __grid_constan
             const int r = j * 128 + row;
             const int x = x0 + r % TX, y = y0 + (r / TX) % TY, z = z0 + r / (TX * TY);
             const size_t vox = ((size_t)z * Y + y) * X + x;
-            const bool valid = z < Z;  // a box may extend past a volume smaller than 128 voxels
-            if (a.epilogue == kEpiComplexOut || a.epilogue == kEpiLossGrad) {
-                float v[8];
-                tmem_ld8(lane_addr + j * COUT, v);
-                tmem_wait_ld();
-                if (!valid) continue;
-                const float f0 = v[0] + (a.bias ? a.bias[0] : 0.f), f1 = v[1] + (a.bias ? a.bias[1] : 0.f);
-                const size_t e = (size_t)n * plane + vox;
-                const float2 in = a.res[e];
-                const float s = a.scale[n];
-                if (a.epilogue == kEpiComplexOut) {
-                    a.out_c[e] = make_float2(in.x + s * f0, in.y + s * f1);
-                } else {
-                    const float2 tg = a.target[e];
-                    const float inv = 1.f / s;
-                    const float d0 = in.x * inv + f0 - tg.x * inv, d1 = in.y * inv + f1 - tg.y * inv;
-                    loss += d0 * d0 + d1 * d1;
-                    float g[8] = {a.grad_scale * d0, a.grad_scale * d1, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                    uint4* o = reinterpret_cast<uint4*>(a.out) + ((size_t)n * a.out_cb_total + a.out_cb_offset) * plane + vox;
-                    o[0] = pack_bf16x8(g);
-                    for (int q = 1; q < COUT / 8; ++q) o[(size_t)q * plane] = make_uint4(0, 0, 0, 0);
-                }
-                continue;
-            }
-#pragma unroll 1
-            for (int q = 0; q < COUT / 8; ++q) {
-                float v[8];
-                tmem_ld8(lane_addr + j * COUT + q * 8, v);
-                tmem_wait_ld();
-                if (!valid) continue;
-                if (a.epilogue == kEpiMask) {
-                    const uint4 m = reinterpret_cast<const uint4*>(
-                        a.mask)[((size_t)n * a.mask_cb_total + a.mask_cb_offset + q) * plane + vox];
-                    float mf[8];
-                    unpack_bf16x8(m, mf);
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) v[i] = mf[i] > 0.f ? v[i] : 0.f;
-                } else {
-                    if (a.bias) {
-#pragma unroll
-                        for (int i = 0; i < 8; ++i) v[i] += __ldg(a.bias + q * 8 + i);
-                    }
-                    if (a.epilogue == kEpiBiasRelu) {
-#pragma unroll
-                        for (int i = 0; i < 8; ++i) v[i] = fmaxf(v[i], 0.f);
-                    }
-                }
-                reinterpret_cast<uint4*>(a.out)[((size_t)n * a.out_cb_total + a.out_cb_offset + q) * plane + vox] =
-                    pack_bf16x8(v);
-            }
+            // a box may extend past a volume smaller than 128 voxels
+            conv_epilogue_voxel<COUT>(a, lane_addr + j * COUT, n, vox, z < Z, plane, loss);
         }
-        if (a.epilogue == kEpiLossGrad) {
-#pragma unroll
-            for (int o = 16; o; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
-            if (lane == 0) atomicAdd(a.loss, loss);
-        }
+        flush_loss(a, loss, lane);
     }
+    if (abort_s) drain_after_abort();
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, C::kTmemCols);
+}
+
+// ---- forward, 128-voxel lines with a shared halo --------------------------------------------
+// For volumes 128 voxels wide. A tile is 2 x 2 (y, z) lines of 128 voxels: four M = 128 MMAs per
+// tap. One TMA box brings the tile's halo -- 130 x 4 x 4 voxels (x, y, z) of two input channel
+// blocks -- into shared memory, and all 27 taps read that one box at voxel offsets
+// ((z + kz) * 4 + y + ky) * 130 + kx (every row stays 16-byte aligned and the 8-row core-matrix
+// stride stays 128 bytes), so an input voxel crosses L2 4x per layer instead of 27x. A stage is
+// (tile, pair of input channel blocks): the halo plus that pair's weights for all taps. Warp 4
+// issues the TMA loads, warp 5 the MMAs, warps 0-3 run the epilogue and hand the accumulators
+// back through a TMEM-empty barrier; CTAs are persistent over tiles.
+template <int CB_IN, int COUT>
+struct LineCfg {
+    static constexpr int kTY = 2, kTZ = 2, kMT = kTY * kTZ;
+    static constexpr int kHX = 130, kHY = kTY + 2, kHZ = kTZ + 2;
+    static constexpr uint32_t kHaloPlane = 16u * kHX * kHY * kHZ;  // one channel block
+    static constexpr uint32_t kHaloBytes = 2 * kHaloPlane;
+    static constexpr uint32_t kWTap = 2u * COUT * 16;                // one tap, two channel blocks
+    static constexpr uint32_t kWBytes = 27 * kWTap;
+    static constexpr uint32_t kStageBytes = kHaloBytes + kWBytes;
+    static constexpr int kStages = 2;
+    static constexpr int kKSteps = CB_IN / 2;
+    static constexpr uint32_t kTmemCols = tmem_cols_for(kMT * COUT);
+    static constexpr uint32_t kSmem = kStages * kStageBytes;
+    static constexpr int kThreads = 192;
+    static_assert(kSmem <= 220u * 1024, "stage ring too large");
+    static_assert(CB_IN % 2 == 0 && COUT % 16 == 0 && kMT * COUT <= 256, "shape");
+};
+
+template <int CB_IN, int COUT>
+__global__ void __launch_bounds__(192, 1) conv_fwd_line_kernel(const __grid_constant__ CUtensorMap tmap,
+                                                               const ConvFwdArgs a, int ntiles)
+{
+    using C = LineCfg<CB_IN, COUT>;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ uint64_t full[C::kStages], empty[C::kStages], accum_full, tmem_empty;
+    __shared__ uint32_t tmem_base_s;
+    __shared__ volatile int abort_s;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int Y = a.shape.Y, Z = a.shape.Z;
+    const int tiles_y = Y / C::kTY, tiles_z = Z / C::kTZ;
+
+    if (tid == 0) {
+        for (int s = 0; s < C::kStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&accum_full, 1);
+        mbar_init(&tmem_empty, 128);
+        abort_s = 0;
+        fence_mbar_init();
+        prefetch_tensormap(&tmap);
+    }
+    if (warp == 0) {
+        tmem_alloc(&tmem_base_s, C::kTmemCols);
+        tmem_relinquish();
+    }
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = tmem_base_s;
+
+    if (warp == 4) {
+        if (lane == 0) {
+            int g = 0;
+            for (int tile = blockIdx.x; tile < ntiles && !abort_s; tile += gridDim.x) {
+                int t = tile;
+                const int iy = t % tiles_y;
+                t /= tiles_y;
+                const int iz = t % tiles_z;
+                const int n = t / tiles_z;
+                for (int ks = 0; ks < C::kKSteps; ++ks, ++g) {
+                    const int slot = g % C::kStages;
+                    if (g >= C::kStages && !mbar_wait(&empty[slot], ((g / C::kStages) - 1) & 1)) {
+                        record_failure(a.status, kFailProducer | 0x40);
+                        abort_s = 1;
+                        break;
+                    }
+                    uint8_t* st = smem + slot * C::kStageBytes;
+                    mbar_arrive_expect_tx(&full[slot], C::kStageBytes);
+                    tma_load_5d(st, &tmap, 0, -1, iy * C::kTY - 1, iz * C::kTZ - 1, n * CB_IN + 2 * ks, &full[slot]);
+                    for (int tap = 0; tap < 27; ++tap)
+                        bulk_load(st + C::kHaloBytes + tap * C::kWTap, a.wf + ((size_t)tap * CB_IN + 2 * ks) * COUT * 8,
+                                  C::kWTap, &full[slot]);
+                }
+            }
+        }
+    } else if (warp == 5) {
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_bf16(128, COUT, false, false);
+            int g = 0, i = 0;
+            for (int tile = blockIdx.x; tile < ntiles && !abort_s; tile += gridDim.x, ++i) {
+                if (i > 0 && !mbar_wait(&tmem_empty, (i - 1) & 1)) {
+                    record_failure(a.status, kFailMma | 0x41);
+                    abort_s = 1;
+                    break;
+                }
+                fence_after_sync();
+                for (int ks = 0; ks < C::kKSteps; ++ks, ++g) {
+                    const int slot = g % C::kStages;
+                    if (!mbar_wait(&full[slot], (g / C::kStages) & 1)) {
+                        record_failure(a.status, kFailMma | 0x40);
+                        abort_s = 1;
+                        break;
+                    }
+                    fence_after_sync();
+                    const uint32_t halo = saddr(smem + slot * C::kStageBytes);
+                    const uint32_t wts = halo + C::kHaloBytes;
+                    for (int tap = 0; tap < 27; ++tap) {
+                        const int kz = tap / 9, ky = (tap / 3) % 3, kx = tap % 3;
+                        const uint64_t bd = smem_desc(wts + tap * C::kWTap, 16 * COUT, 128);
+#pragma unroll
+                        for (int j = 0; j < C::kMT; ++j) {
+                            const int zl = j / C::kTY, yl = j % C::kTY;
+                            const uint32_t start = halo + (((zl + kz) * C::kHY + (yl + ky)) * C::kHX + kx) * 16;
+                            const uint64_t ad = smem_desc(start, C::kHaloPlane, 128);
+                            mma_bf16(tmem + j * COUT, ad, bd, idesc, (ks | tap) != 0);
+                        }
+                    }
+                    mma_commit(&empty[slot]);
+                }
+                if (abort_s) break;
+                mma_commit(&accum_full);
+            }
+        }
+    } else {
+        // epilogue: warps 0-3, TMEM lanes 32 * warp + lane = x of a 128-voxel line
+        const size_t plane = (size_t)128 * Y * Z;
+        const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
+        const int x = 32 * warp + lane;
+        float loss = 0.f;
+        int i = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
+            const bool ok = __all_sync(0xffffffffu, mbar_wait(&accum_full, i & 1));
+            if (!ok || abort_s) {
+                if (lane == 0 && !ok) record_failure(a.status, kFailEpilogue | 0x40);
+                abort_s = 1;
+                break;
+            }
+            fence_after_sync();
+            int t = tile;
+            const int iy = t % tiles_y;
+            t /= tiles_y;
+            const int iz = t % tiles_z;
+            const int n = t / tiles_z;
+#pragma unroll 1
+            for (int j = 0; j < C::kMT; ++j) {
+                const int z = iz * C::kTZ + j / C::kTY, y = iy * C::kTY + j % C::kTY;
+                conv_epilogue_voxel<COUT>(a, lane_addr + j * COUT, n, ((size_t)z * Y + y) * 128 + x, true, plane, loss);
+            }
+            fence_before_sync();
+            mbar_arrive(&tmem_empty);
+        }
+        flush_loss(a, loss, lane);
+    }
+    __syncwarp();
+    __syncthreads();
     if (abort_s) drain_after_abort();
     fence_before_sync();
     __syncthreads();
@@ -389,6 +565,7 @@ __global__ void __launch_bounds__(kThreads) conv_wgrad_kernel(const __grid_const
 
 // ---- host: tensor maps and dispatch ----------------------------------------------------------
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+bool g_force_tap_kernel = false;  // test hook: always use the per-tap forward kernel
 std::mutex g_encode_mutex;
 
 bool encode_fn(PFN_cuTensorMapEncodeTiled_v12000* out)
@@ -461,8 +638,39 @@ bool launch_fwd(const ConvFwdArgs& a, cudaStream_t st)
 }
 
 template <int CB_IN, int COUT>
+bool launch_fwd_line(const ConvFwdArgs& a, cudaStream_t st)
+{
+    using C = LineCfg<CB_IN, COUT>;
+    CUtensorMap map;
+    if (!c8_tensor_map(&map, a.in, a.shape, CB_IN, C::kHX, C::kHY, C::kHZ, 2)) return false;
+    auto k = conv_fwd_line_kernel<CB_IN, COUT>;
+    CUTB_CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::kSmem));
+    const int ntiles = a.shape.NB * (a.shape.Y / C::kTY) * (a.shape.Z / C::kTZ);
+    int sms = 148;
+    {
+        int dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    const int grid = ntiles < sms ? ntiles : sms;
+    k<<<grid, C::kThreads, C::kSmem, st>>>(map, a, ntiles);
+    CUTB_CUDA_OK(cudaGetLastError());
+    return true;
+}
+
+// The halo kernel serves 128-wide volumes whose weights for all taps of two channel blocks fit
+// its stage (cout <= 32); everything else uses the per-tap kernel.
+template <int CB_IN, int COUT>
+constexpr bool line_kernel_fits()
+{
+    return COUT <= 32 && CB_IN % 2 == 0 && CB_IN <= 8;
+}
+
+template <int CB_IN, int COUT>
 bool dispatch_fwd_mt(const ConvFwdArgs& a, cudaStream_t st)
 {
+    if constexpr (line_kernel_fits<CB_IN, COUT>())
+        if (a.shape.X == 128 && a.shape.Y % 2 == 0 && a.shape.Z % 2 == 0 && !g_force_tap_kernel)
+            return launch_fwd_line<CB_IN, COUT>(a, st);
     const long long vox = (long long)a.shape.X * a.shape.Y * a.shape.Z;
     int TX, TY, TZ;
     if constexpr (4 * COUT <= 256 && 16u * 512 * CB_IN <= 64u * 1024)
@@ -651,6 +859,8 @@ unsigned grid_for(size_t work, int threads = 256)
 }
 
 }  // namespace
+
+void conv3d_force_tap_kernel(bool on) { g_force_tap_kernel = on; }
 
 bool conv3d_forward(const ConvFwdArgs& a, cudaStream_t st)
 {

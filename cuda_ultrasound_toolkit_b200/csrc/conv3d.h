@@ -62,6 +62,8 @@ struct ConvWgradArgs {
 };
 
 bool conv3d_forward(const ConvFwdArgs& a, cudaStream_t stream);
+// Test hook: route every forward convolution through the per-tap kernel.
+void conv3d_force_tap_kernel(bool on);
 bool conv3d_wgrad(const ConvWgradArgs& a, cudaStream_t stream);
 
 // Helpers on C8 volumes (all BF16 unless noted).

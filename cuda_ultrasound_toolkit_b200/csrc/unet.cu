@@ -489,6 +489,8 @@ CUTB_API bool cutb_unet_check(cutb_unet* net)
 }
 
 // ---- single convolutions (tests and tools) ---------------------------------------------------
+CUTB_API void cutb_debug_conv3d_force_tap_kernel(int on) { conv3d_force_tap_kernel(on != 0); }
+
 CUTB_API bool cutb_conv3d_relayout(const float* d_w, unsigned cin, unsigned cout, void* d_wf, void* d_wb, void* stream)
 {
     CUTB_REQUIRE(d_w && d_wf && d_wb && cin % 16 == 0 && cout % 16 == 0 && cin && cout, CUTB_ERR_INVALID_ARGUMENT,

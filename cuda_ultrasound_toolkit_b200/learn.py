@@ -40,6 +40,7 @@ def _lib():
             "cutb_conv3d_relayout": ([vp, u, u, vp, vp, vp], b),
             "cutb_conv3d_forward": ([vp, vp, vp, vp, u, u, u, u, u, u, ctypes.c_int, vp, vp], b),
             "cutb_conv3d_weight_grad": ([vp, vp, vp, u, u, u, u, u, u, vp, vp], b),
+            "cutb_debug_conv3d_force_tap_kernel": ([ctypes.c_int], None),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -92,6 +93,11 @@ def conv3d(x_c8, wf, bias, cout, relu=False, status=None, stream=None):
                                       out.data_ptr(), X, Y, Z, n, CB * 8, cout, int(relu), st.data_ptr(),
                                       _stream_handle(stream)), "cutb_conv3d_forward")
     return out
+
+
+def force_tap_kernel(on):
+    """Test hook: route every forward convolution through the per-tap kernel."""
+    _lib().cutb_debug_conv3d_force_tap_kernel(int(bool(on)))
 
 
 def conv3d_weight_grad(x_c8, dout_c8, status=None, stream=None):

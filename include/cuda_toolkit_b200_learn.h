@@ -86,6 +86,8 @@ CUTB_API bool cutb_conv3d_relayout(const float* d_w, uint cin, uint cout, void* 
 CUTB_API bool cutb_conv3d_forward(const void* d_in, const void* d_wf, const float* d_bias, void* d_out, uint X,
                                   uint Y, uint Z, uint nb, uint cin, uint cout, int relu, int* d_status,
                                   void* stream);
+/* Test hook: 1 routes every forward convolution through the per-tap kernel (no halo reuse). */
+CUTB_API void cutb_debug_conv3d_force_tap_kernel(int on);
 CUTB_API bool cutb_conv3d_weight_grad(const void* d_in, const void* d_dout, float* d_dw, uint X, uint Y, uint Z,
                                       uint nb, uint cin, uint cout, int* d_status, void* stream);
 

@@ -47,7 +47,28 @@ CONV_CASES = [
     (32, 128, 4, 8, 8, 1),
     (16, 16, 4, 4, 4, 1),      # smaller than one 128-voxel tile
     (64, 16, 16, 8, 16, 2),
+    # 128-wide volumes: the halo kernel (two channel blocks per stage, cout <= 32)
+    (32, 16, 4, 8, 128, 2),
+    (16, 32, 2, 2, 128, 1),
+    (64, 16, 2, 4, 128, 1),
 ]
+
+
+@pytest.mark.parametrize("cin,cout,Z,Y,X,n", [c for c in CONV_CASES if c[4] == 128])
+def test_conv3d_halo_kernel_matches_tap_kernel(cin, cout, Z, Y, X, n):
+    """The halo kernel and the per-tap kernel compute the same sums (FP32 accumulation order may differ)."""
+    g = torch.Generator().manual_seed(cin + cout + Z + Y)
+    x = bf16_exact(n, cin, Z, Y, X, gen=g)
+    w = bf16_exact(cout, cin, 3, 3, 3, gen=g, scale=(1.0 / (27 * cin)) ** 0.5)
+    wf, _ = learn.relayout(learn.master_weight(w).float().cuda(), cin, cout)
+    xc = learn.to_c8(x.float().cuda())
+    a = learn.from_c8(learn.conv3d(xc, wf, None, cout)).float()
+    learn.force_tap_kernel(True)
+    try:
+        b = learn.from_c8(learn.conv3d(xc, wf, None, cout)).float()
+    finally:
+        learn.force_tap_kernel(False)
+    assert rel_l2(a.cpu(), b.cpu()) < 4e-3
 
 
 @pytest.mark.parametrize("cin,cout,Z,Y,X,n", CONV_CASES)
@@ -112,7 +133,7 @@ def _unet_case(shape, seed, nb=1):
     return net, p, vol.astype(np.complex64), tgt.astype(np.complex64)
 
 
-@pytest.mark.parametrize("shape,nb", [((16, 16, 16), 1), ((32, 32, 32), 2), ((16, 32, 64), 1)])
+@pytest.mark.parametrize("shape,nb", [((16, 16, 16), 1), ((32, 32, 32), 2), ((16, 32, 64), 1), ((16, 16, 128), 2)])
 def test_unet_forward_matches_reference(shape, nb):
     from oracle import unet_ref
     net, p, vol, _ = _unet_case(shape, 11, nb)
@@ -124,7 +145,7 @@ def test_unet_forward_matches_reference(shape, nb):
     assert rel_l2(torch.from_numpy(out - vol), ref - torch.from_numpy(vol).to(torch.complex128)) < 3e-2
 
 
-@pytest.mark.parametrize("shape,nb", [((16, 16, 16), 1), ((32, 32, 32), 2)])
+@pytest.mark.parametrize("shape,nb", [((16, 16, 16), 1), ((32, 32, 32), 2), ((16, 16, 128), 1)])
 def test_unet_gradients_match_reference(shape, nb):
     from oracle import unet_ref
     net, p, vol, tgt = _unet_case(shape, 5, nb)
