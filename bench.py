@@ -312,6 +312,11 @@ def run_ours(args, rank, world, local_rank):
     }
     if args.learned > 0 and world == 1:
         line["learned"] = learned_path(args.learned)
+    if args.batched > 0 and world == 1:
+        try:
+            line["batched"] = batched_stream(args.batched)
+        except Exception as exc:  # must not hide the plain pipeline's number
+            line["batched"] = {"failed": str(exc)}
     try:
         per_vol, sample = cpu_sample(frames[0][0], bp, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": 1.0 / per_vol, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
@@ -345,6 +350,66 @@ def learned_path(volumes):
         return {"failed": str(exc)}
 
 
+def batched_stream(n_frames, seed=4):
+    """Config 4: a seeded stream of frames of mixed size (transmits 32/64/128, channels 64/128,
+    samples 1024-8192, volumes 64^3 / 128^2 x 128 / 128^2 x 256), simulated on the GPU. Times the
+    frame-by-frame path (per-frame plans: decode, Hilbert, delay-and-sum launches) against one
+    cutb_batch run replayed from its CUDA graph (front ends + one persistent delay-and-sum per
+    kernel variant), tile shapes from the autotuner, inputs resident in HBM."""
+    import torch
+    from cuda_ultrasound_toolkit_b200 import Batch, Plan, batched
+    from cuda_ultrasound_toolkit_b200.tune import DasTuner
+    specs = batched.frame_specs(seed, n_frames)
+    frames = batched.make_frames(specs)
+    params = [bp for _, bp in frames]
+    raws = [r for r, _ in frames]
+    t0 = time.perf_counter()
+    tuner = DasTuner(reps=2)
+    tiles = [tuner.choose(bp) for bp in params]
+    tuning_s = time.perf_counter() - t0
+    plans = [Plan(bp, das_tile=t) for bp, t in zip(params, tiles)]
+    n_dec = max(p.empty_decoded().numel() for p in plans)
+    dec = torch.empty(n_dec, dtype=torch.float32, device="cuda")
+    iq = torch.empty(n_dec, dtype=torch.complex64, device="cuda")
+    batch = Batch(params, das_tiles=tiles)
+    vols = batch.empty_volumes()
+
+    def loop():
+        for p, r, v in zip(plans, raws, vols):
+            S, C, T = p.bp.dims
+            d = dec[:T * C * S].view(T, C, S)
+            q = iq[:T * C * S].view(T, C, S)
+            p.decode(r, out=d)
+            p.hilbert(d, out=q)
+            p.das(q, out=v)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    loop_ms = timed(loop, 2)
+    for p in plans:
+        p.check()
+    batch_ms = timed(lambda: batch.run(raws, vols, graph=True), 3)
+    batch.check()
+    work = batched.work(params)
+    return {"frames": n_frames, "seed": seed, "voxel_transmit_channel": work,
+            "frame_loop": {"ms": loop_ms, "volumes_per_s": 1e3 * n_frames / loop_ms,
+                           "launches": 3 * n_frames},
+            "batched_graph": {"ms": batch_ms, "volumes_per_s": 1e3 * n_frames / batch_ms,
+                              "launches": batch.launches_per_run, "das_launches": batch.das_launches,
+                              "vct_per_s": work / (batch_ms * 1e-3)},
+            "speedup": loop_ms / batch_ms, "tile_choice": {str(t): tiles.count(t) for t in set(tiles)},
+            "tuning_seconds": tuning_s}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -353,6 +418,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--learned", type=int, default=16,
                     help="held-out volumes for the learned sparse-transmit path (0: skip)")
+    ap.add_argument("--batched", type=int, default=64, help="frames of the batched mixed-size stream (0: skip)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -7,11 +7,11 @@ kernels); this package is its Python host mirror. There is no CPU fallback.
 """
 from .params import (ApoType, CudaBeamformerParameters, EncodingMatrix, InputDataTypes, RCAOrientation,
                      SampleType, SequenceId)
-from .api import (CutbError, Plan, RfSession, beamform, beamform_f32, beamform_i16, encoding_matrix, last_error,
+from .api import (Batch, CutbError, Plan, RfSession, beamform, beamform_f32, beamform_i16, encoding_matrix, last_error,
                   lib, library_path)
 
 __all__ = [
     "ApoType", "CudaBeamformerParameters", "EncodingMatrix", "InputDataTypes", "RCAOrientation", "SampleType",
-    "SequenceId", "CutbError", "Plan", "RfSession", "beamform", "beamform_f32", "beamform_i16", "encoding_matrix",
+    "SequenceId", "Batch", "CutbError", "Plan", "RfSession", "beamform", "beamform_f32", "beamform_i16", "encoding_matrix",
     "last_error", "lib", "library_path",
 ]

@@ -67,6 +67,12 @@ def lib():
         "cutb_calibrate_fp32": ([ctypes.POINTER(ctypes.c_double), vp], b),
         "cutb_plan_check": ([vp, vp], b),
         "cutb_plan_das_tile_shape": ([vp, ctypes.POINTER(u)], b),
+        "cutb_batch_create": ([P, vp, u], vp),
+        "cutb_batch_destroy": ([vp], None),
+        "cutb_batch_run": ([vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_int, vp], b),
+        "cutb_batch_check": ([vp, vp], b),
+        "cutb_batch_launches_per_run": ([vp], ctypes.c_int),
+        "cutb_batch_das_launches": ([vp], ctypes.c_int),
         "cutb_das_tiles": ([vp, vp, vp, ctypes.POINTER(ctypes.c_int), u, u, vp], b),
         "init_cuda_configuration": ([ctypes.POINTER(u), ctypes.POINTER(u)], b),
         "register_cuda_buffers": ([ctypes.POINTER(u), u, u], b),
@@ -252,6 +258,52 @@ class Plan:
         _check(lib().cutb_beamform(self._h, raw.data_ptr(), raw.numel() * raw.element_size(), out.data_ptr(),
                                    _stream_handle(stream)), "cutb_beamform")
         return out
+
+
+class Batch:
+    """cutb_batch: many frames of uneven size beamformed with one persistent delay-and-sum launch
+    per kernel variant, optionally replayed from a captured CUDA graph."""
+
+    def __init__(self, params, das_tiles=None):
+        n = len(params)
+        self._bps = (CudaBeamformerParameters * n)(*[bp.copy() for bp in params])
+        opts = None
+        if das_tiles is not None:
+            opts = (_Options * n)(*[_Options(0, int(t)) for t in das_tiles])
+        self._h = lib().cutb_batch_create(self._bps, opts, n)
+        _check(self._h, "cutb_batch_create")
+        self.n = n
+        self.shapes = [bp.volume_shape for bp in params]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cutb_batch_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    @property
+    def launches_per_run(self):
+        return lib().cutb_batch_launches_per_run(self._h)
+
+    @property
+    def das_launches(self):
+        return lib().cutb_batch_das_launches(self._h)
+
+    def empty_volumes(self):
+        import torch
+        return [torch.empty(s, dtype=torch.complex64, device="cuda") for s in self.shapes]
+
+    def run(self, raws, volumes=None, graph=False, stream=None):
+        volumes = self.empty_volumes() if volumes is None else volumes
+        assert len(raws) == self.n and len(volumes) == self.n
+        rp = (ctypes.c_void_p * self.n)(*[r.data_ptr() for r in raws])
+        vp_ = (ctypes.c_void_p * self.n)(*[v.data_ptr() for v in volumes])
+        _check(lib().cutb_batch_run(self._h, rp, vp_, int(graph), _stream_handle(stream)), "cutb_batch_run")
+        return volumes
+
+    def check(self, stream=None):
+        _check(lib().cutb_batch_check(self._h, _stream_handle(stream)), "cutb_batch_check")
 
 
 # ---- buffer-registry front end ------------------------------------------------------------------

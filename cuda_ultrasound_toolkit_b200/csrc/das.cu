@@ -89,6 +89,10 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
                  "l"(src), "r"(bytes), "r"(smem_addr(bar))
                  : "memory");
 }
+__device__ __forceinline__ void mbar_inval(uint64_t* bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
@@ -463,29 +467,17 @@ struct Layout {
     static constexpr int TZ = (kShort ? 2 : kWarps) * kVpt;
 };
 
+// One tile (bx, by, bz) of the volume, stage slice `split` of a.splits. Called by the grid
+// kernel (a in parameter space) and by the persistent batch kernel (a in its parameter table).
 template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT>
-__global__ void __launch_bounds__(kThreads, 3)
-das_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
+__device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __restrict__ vol, const DasArgs& a,
+                                         Smem<IQ, CUBIC>& sm, int bx, int by, int bz, int split)
 {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    auto& sm = *reinterpret_cast<Smem<IQ, CUBIC>*>(smem_raw);
     constexpr bool HERC = SEQ == HERCULES;
     using L = Layout<SEQ, SHORT>;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
     // ---- tile, voxels, offsets from the tile centre -----------------------------------------
-    // Whole grid: blockIdx.xyz is the tile. Tile list: blockIdx.x indexes a.tiles and
-    // blockIdx.y is the slice of the stages (transmits x channel groups) this CTA sums.
-    int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
-    int split = 0;
-    if (a.tiles) {
-        const int nx = div_up(a.X, L::TX), ny = div_up(a.Y, L::TY);
-        const int id = a.tiles[blockIdx.x];
-        bx = id % nx;
-        by = (id / nx) % ny;
-        bz = id / (nx * ny);
-        split = blockIdx.y;
-    }
     const int tx0 = bx * L::TX, ty0 = by * L::TY, tz0 = bz * L::TZ;
     const float ix_c = tx0 + 0.5f * (L::TX - 1), iy_c = ty0 + 0.5f * (L::TY - 1), iz_c = tz0 + 0.5f * (L::TZ - 1);
     Tile tile;
@@ -653,6 +645,57 @@ das_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
     }
 }
 
+// Whole grid: blockIdx.xyz is the tile. Tile list: blockIdx.x indexes a.tiles and blockIdx.y
+// is the slice of the stages (transmits x channel groups) this CTA sums.
+template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT>
+__global__ void __launch_bounds__(kThreads, 3)
+das_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    auto& sm = *reinterpret_cast<Smem<IQ, CUBIC>*>(smem_raw);
+    using L = Layout<SEQ, SHORT>;
+    int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
+    int split = 0;
+    if (a.tiles) {
+        const int nx = div_up(a.X, L::TX), ny = div_up(a.Y, L::TY);
+        const int id = a.tiles[blockIdx.x];
+        bx = id % nx;
+        by = (id / nx) % ny;
+        bz = id / (nx * ny);
+        split = blockIdx.y;
+    }
+    das_tile<SEQ, CUBIC, CF, APO, IQ, SHORT>(iq, vol, a, sm, bx, by, bz, split);
+}
+
+// Persistent delay-and-sum over the tiles of many frames: CTAs take (frame, tile) work items,
+// heaviest first, from a device counter until the list is exhausted. Frame arguments sit in the
+// kernel's parameter table (uniform per CTA, read through the constant cache).
+template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT>
+__global__ void __launch_bounds__(kThreads, 3)
+das_batch_kernel(const DasBatchParams P, const int2* __restrict__ items, int nitems, int* __restrict__ counter)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    auto& sm = *reinterpret_cast<Smem<IQ, CUBIC>*>(smem_raw);
+    using L = Layout<SEQ, SHORT>;
+    __shared__ int item_s;
+    for (;;) {
+        if (threadIdx.x == 0) item_s = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = item_s;
+        if (it >= nitems) break;
+        const int2 w = items[it];
+        const DasFrame& f = P.f[w.x];
+        const int nx = div_up(f.a.X, L::TX), ny = div_up(f.a.Y, L::TY);
+        das_tile<SEQ, CUBIC, CF, APO, IQ, SHORT>((const IQ*)f.iq, f.vol, f.a, sm, w.y % nx, (w.y / nx) % ny,
+                                                 w.y / (nx * ny), 0);
+        __syncthreads();
+        if (sm.abort) break;
+        if (threadIdx.x == 0)
+            for (int b = 0; b < kStages; ++b) mbar_inval(&sm.full[b]);
+        __syncthreads();
+    }
+}
+
 template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT>
 bool launch_das_t(const DasArgs& a, const void* iq, void* volume, cudaStream_t st)
 {
@@ -805,6 +848,67 @@ bool derive_das(const CudaBeamformerParameters& bp, DasArgs& a)
 static bool use_short_tile(const DasArgs& a)
 {
     return a.seq == HERCULES && (a.tile == 2 || (a.tile == 0 && prefer_short_tile(a)));
+}
+
+bool das_uses_short_tile(const DasArgs& a) { return use_short_tile(a); }
+
+namespace {
+// grid > 0: launch with that many persistent CTAs; grid == 0: only prepare the kernel (shared
+// memory attribute) and return its resident CTAs per SM in *per_sm.
+template <bool CUBIC, bool CF, bool APO, class IQ, bool SHORT>
+bool launch_batch_t(const DasBatchParams* P, const int2* items, int nitems, int* counter, int grid, int* per_sm,
+                    cudaStream_t st)
+{
+    auto kern = das_batch_kernel<HERCULES, CUBIC, CF, APO, IQ, SHORT>;
+    const size_t smem = sizeof(Smem<IQ, CUBIC>);
+    if (grid <= 0) {
+        CUTB_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CUTB_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kern, kThreads, smem));
+        return true;
+    }
+    kern<<<grid, kThreads, smem, st>>>(*P, items, nitems, counter);
+    CUTB_CUDA_OK(cudaGetLastError());
+    return true;
+}
+
+template <class IQ, bool SHORT>
+bool launch_batch_s(const DasBatchParams* P, const int2* items, int nitems, int* counter, const DasArgs& a, int grid,
+                    int* per_sm, cudaStream_t st)
+{
+#define CUTB_BATCH_CASE(CUBIC, CF, APO)                                                 \
+    if ((bool)a.cubic == CUBIC && (bool)a.apply_cf == CF && (bool)a.use_apo == APO) \
+        return launch_batch_t<CUBIC, CF, APO, IQ, SHORT>(P, items, nitems, counter, grid, per_sm, st);
+    CUTB_BATCH_CASE(true, true, false)
+    CUTB_BATCH_CASE(true, false, false)
+    CUTB_BATCH_CASE(false, true, false)
+    CUTB_BATCH_CASE(false, false, false)
+    CUTB_BATCH_CASE(true, true, true)
+    CUTB_BATCH_CASE(true, false, true)
+    CUTB_BATCH_CASE(false, true, true)
+    CUTB_BATCH_CASE(false, false, true)
+#undef CUTB_BATCH_CASE
+    return false;
+}
+}  // namespace
+
+bool launch_das_batch(const DasBatchParams* P, const int2* items, int nitems, int* counter, const DasArgs& like,
+                      bool iq_bf16, bool short_tile, int grid, int* per_sm, cudaStream_t st)
+{
+    CUTB_REQUIRE(like.seq == HERCULES, CUTB_ERR_UNSUPPORTED, "Batched delay-and-sum supports HERCULES frames.");
+    CUTB_REQUIRE(grid <= 0 || (nitems > 0 && items && counter && P), CUTB_ERR_INVALID_ARGUMENT, "Empty batch.");
+    CUTB_REQUIRE(grid > 0 || per_sm, CUTB_ERR_INVALID_ARGUMENT, "Missing occupancy output.");
+    if (short_tile)
+        return iq_bf16 ? launch_batch_s<__nv_bfloat162, true>(P, items, nitems, counter, like, grid, per_sm, st)
+                       : launch_batch_s<float2, true>(P, items, nitems, counter, like, grid, per_sm, st);
+    return iq_bf16 ? launch_batch_s<__nv_bfloat162, false>(P, items, nitems, counter, like, grid, per_sm, st)
+                   : launch_batch_s<float2, false>(P, items, nitems, counter, like, grid, per_sm, st);
+}
+
+void das_grid_tiles(const DasArgs& a, int counts[3])
+{
+    int shape[3];
+    das_tile_shape(a, shape);
+    for (int i = 0; i < 3; ++i) counts[i] = div_up(i == 0 ? a.X : i == 1 ? a.Y : a.Z, shape[i]);
 }
 
 void das_tile_shape(const DasArgs& a, int shape[3])

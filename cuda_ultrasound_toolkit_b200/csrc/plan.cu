@@ -350,6 +350,7 @@ CUTB_API bool cutb_beamform(cutb_plan* p, const void* d_raw, size_t raw_bytes, v
     CUTB_REQUIRE(d_raw && d_volume, CUTB_ERR_INVALID_ARGUMENT, "Null device buffer.");
     cudaStream_t st = (cudaStream_t)stream;
     p->launches = 0;
+    if (!p->ensure_buffers()) return false;
     if (!p->fe.decode(d_raw, p->data_type, p->d_decoded, 1, st)) return false;
     if (!p->fe.hilbert(p->d_decoded, 1, p->d_iq, p->iq_bf16, st)) return false;
     p->launches = 2;
@@ -389,11 +390,19 @@ bool cutb_plan::build(const CudaBeamformerParameters& params, const cutb_options
     const size_t samples = (size_t)bp.dec_data_dim[0] * bp.dec_data_dim[1] * bp.dec_data_dim[2];
     iq_bytes = samples * (iq_bf16 ? 4 : 8);
     vol_bytes = (size_t)bp.output_points[0] * bp.output_points[1] * bp.output_points[2] * 8;
-    if (!alloc_bytes((void**)&d_decoded, samples * sizeof(float))) return false;
-    if (!alloc_bytes(&d_iq, iq_bytes)) return false;
+    decoded_bytes = samples * sizeof(float);
     if (!alloc_bytes((void**)&d_status, sizeof(int))) return false;
     CUTB_CUDA_OK(cudaMemset(d_status, 0, sizeof(int)));
     das.status = d_status;
+    return true;
+}
+
+// The intermediate buffers of cutb_beamform, allocated on its first call (plans that only run
+// stages on caller buffers, such as the frames of a batch, never allocate them).
+bool cutb_plan::ensure_buffers()
+{
+    if (!d_decoded && !alloc_bytes((void**)&d_decoded, decoded_bytes)) return false;
+    if (!d_iq && !alloc_bytes(&d_iq, iq_bytes)) return false;
     return true;
 }
 

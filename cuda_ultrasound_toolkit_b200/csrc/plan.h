@@ -41,7 +41,7 @@ struct cutb_plan {
     int data_type = TYPE_I16;
     cutb::FrontEnd fe;
     cutb::DasArgs das{};
-    size_t raw_bytes = 0, iq_bytes = 0, vol_bytes = 0;
+    size_t raw_bytes = 0, iq_bytes = 0, vol_bytes = 0, decoded_bytes = 0;
     float* d_decoded = nullptr;
     void* d_iq = nullptr;
     int* d_status = nullptr;   // device-side error word of the stage kernels
@@ -50,5 +50,6 @@ struct cutb_plan {
     int launches = 0;
 
     bool build(const CudaBeamformerParameters& params, const cutb_options* options);
+    bool ensure_buffers();
     ~cutb_plan();
 };

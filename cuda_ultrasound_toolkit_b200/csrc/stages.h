@@ -76,6 +76,29 @@ struct DasArgs {
     int* status;               // device word: bit 0 set when a bounded wait gave up
 };
 
+// One frame of a persistent batched delay-and-sum: its constants and device buffers.
+struct DasFrame {
+    DasArgs a;
+    const void* iq;
+    float2* vol;
+};
+constexpr int kDasBatchMaxFrames = 96;
+// Passed by value as the kernel's parameter table (< 32 KiB of kernel parameters).
+struct DasBatchParams {
+    DasFrame f[kDasBatchMaxFrames];
+};
+static_assert(sizeof(DasBatchParams) <= 32000, "batched delay-and-sum parameter table too large");
+
+// Launches the persistent delay-and-sum over `nitems` (frame, tile id) items of frames that share
+// sequence, interpolation, coherence, apodization, storage and tile shape with `like`, on `grid`
+// CTAs; `counter` must be zero. With grid <= 0 it only prepares the kernel and reports its resident
+// CTAs per SM (call that once, outside any stream capture).
+bool launch_das_batch(const DasBatchParams* P, const int2* items, int nitems, int* counter, const DasArgs& like,
+                      bool iq_bf16, bool short_tile, int grid, int* per_sm, cudaStream_t st);
+bool das_uses_short_tile(const DasArgs& a);
+// Tiles along x, y, z of the delay-and-sum grid for these arguments.
+void das_grid_tiles(const DasArgs& a, int counts[3]);
+
 // Derives the delay-and-sum constants from the parameter block, applying the same
 // validation as the upstream dispatcher (beamformer.cu:17-197).
 bool derive_das(const CudaBeamformerParameters& bp, DasArgs& a);

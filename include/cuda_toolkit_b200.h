@@ -106,6 +106,25 @@ CUTB_API bool cutb_plan_das_tile_shape(const cutb_plan* plan, uint shape[3]);
 CUTB_API bool cutb_das_tiles(cutb_plan* plan, const void* d_iq, void* d_volume, const int* tiles, uint ntiles,
                              uint splits, void* stream);
 
+/* ---- batched beamforming (no counterpart upstream) --------------------------------------------
+ * Many frames of uneven size (each its own parameter block; HERCULES) beamformed together: every
+ * frame's decode + Hilbert, then one persistent delay-and-sum launch per kernel variant that takes
+ * (frame, tile) work items, heaviest first, from a device counter. Frames with identical blocks
+ * and options share tables; every frame owns its intermediate buffers (allocated here).
+ * cutb_batch_run: d_raw[i] -> d_volume[i] (complex64 [Z][Y][X]); with use_graph the whole run is
+ * captured into a CUDA graph on the first call for a set of pointers and replayed afterwards.
+ * Work runs on the batch's own stream, ordered after and before `stream`. */
+typedef struct cutb_batch cutb_batch;
+CUTB_API cutb_batch* cutb_batch_create(const CudaBeamformerParameters* params, const cutb_options* options,
+                                       uint count);
+CUTB_API void cutb_batch_destroy(cutb_batch* batch);
+CUTB_API bool cutb_batch_run(cutb_batch* batch, const void* const* d_raw, void* const* d_volume, int use_graph,
+                             void* stream);
+/* cutb_plan_check for every frame's plan. */
+CUTB_API bool cutb_batch_check(cutb_batch* batch, void* stream);
+CUTB_API int cutb_batch_launches_per_run(const cutb_batch* batch);
+CUTB_API int cutb_batch_das_launches(const cutb_batch* batch);
+
 /* Synchronises `stream` and reports whether a kernel of this plan hit a bounded device-side
  * wait (CUTB_ERR_TIMEOUT); clears the flag. cuda_toolkit::beamform calls it on every frame. */
 CUTB_API bool cutb_plan_check(cutb_plan* plan, void* stream);

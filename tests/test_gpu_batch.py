@@ -1,0 +1,88 @@
+"""Batched beamforming (cutb_batch: persistent delay-and-sum over many frames, CUDA graph replay)
+and the tile autotuner.
+
+The batch runs the same per-tile code as the single-frame path, so every frame's volume must be
+bit-identical to cutb_beamform of that frame alone, with or without the graph.
+"""
+import numpy as np
+import pytest
+import torch
+
+from cuda_ultrasound_toolkit_b200 import Batch, Plan, batched
+from cuda_ultrasound_toolkit_b200.tune import DasTuner, CANDIDATES
+
+pytestmark = pytest.mark.gpu
+
+SPECS = [
+    dict(T=8, C=8, S=512, X=20, Y=9, Z=40, scatterers=10, seed=1),
+    dict(T=16, C=16, S=1024, X=16, Y=16, Z=24, scatterers=30, seed=2),
+    dict(T=8, C=16, S=512, X=33, Y=3, Z=70, scatterers=12, seed=3),     # partial tiles in every direction
+    dict(T=16, C=8, S=1024, X=12, Y=12, Z=12, scatterers=5, seed=4),
+    dict(T=8, C=8, S=512, X=20, Y=9, Z=40, scatterers=17, seed=5),       # same parameters as frame 0
+    dict(T=32, C=16, S=2048, X=24, Y=16, Z=64, scatterers=40, seed=6),
+]
+
+
+@pytest.fixture(scope="module")
+def frames():
+    return batched.make_frames(SPECS)
+
+
+def reference(frames, tiles=None):
+    out = []
+    for k, (raw, bp) in enumerate(frames):
+        plan = Plan(bp, das_tile=0 if tiles is None else tiles[k])
+        out.append(plan.beamform(raw))
+        plan.check()
+    return out
+
+
+def test_batch_equals_single_frames(frames):
+    b = Batch([bp for _, bp in frames])
+    vols = b.run([r for r, _ in frames])
+    b.check()
+    for v, ref in zip(vols, reference(frames)):
+        assert torch.equal(v, ref)
+    assert b.launches_per_run == 2 * len(frames) + b.das_launches
+    assert 1 <= b.das_launches <= 2
+
+
+def test_batch_graph_replay(frames):
+    b = Batch([bp for _, bp in frames])
+    raws = [r for r, _ in frames]
+    vols = b.empty_volumes()
+    ref = [v.clone() for v in b.run(raws, vols)]
+    for _ in range(3):
+        for v in vols:
+            v.zero_()
+        b.run(raws, vols, graph=True)
+        b.check()
+        for v, r in zip(vols, ref):
+            assert torch.equal(v, r)
+    # new output buffers: the graph is captured again for the new pointers
+    vols2 = b.run(raws, graph=True)
+    b.check()
+    for v, r in zip(vols2, ref):
+        assert torch.equal(v, r)
+
+
+def test_batch_mixed_tiles(frames):
+    tiles = [1, 2, 2, 1, 2, 1]
+    b = Batch([bp for _, bp in frames], das_tiles=tiles)
+    assert b.das_launches == 2
+    vols = b.run([r for r, _ in frames], graph=True)
+    b.check()
+    for v, ref in zip(vols, reference(frames, tiles)):
+        assert torch.equal(v, ref)
+
+
+def test_tuner_choice_is_fastest_on_remeasure(tmp_path):
+    spec = dict(T=32, C=64, S=2048, X=64, Y=64, Z=64, scatterers=50, seed=9)
+    bp = batched.make_frames([spec])[0][1]
+    tuner = DasTuner(str(tmp_path / "tiles.json"), reps=3)
+    best = tuner.choose(bp)
+    times = {t: tuner.measure(bp, t, reps=5) for t in CANDIDATES}
+    assert times[best] <= 1.1 * min(times.values()), times
+    # persisted and reloaded without measuring again
+    again = DasTuner(str(tmp_path / "tiles.json"))
+    assert again.choose(bp) == best
