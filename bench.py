@@ -312,6 +312,11 @@ def run_ours(args, rank, world, local_rank):
     }
     if args.learned > 0 and world == 1:
         line["learned"] = learned_path(args.learned)
+    if args.precision and world == 1:
+        try:
+            line["precision"] = precision_form()
+        except Exception as exc:  # must not hide the plain pipeline's number
+            line["precision"] = {"failed": str(exc)}
     if args.batched > 0 and world == 1:
         try:
             line["batched"] = batched_stream(args.batched)
@@ -410,6 +415,68 @@ def batched_stream(n_frames, seed=4):
             "tuning_seconds": tuning_s}
 
 
+def precision_form(seed=3000):
+    """Config 3: 256 transmits x 256 channels x 8192 samples (1 GiB of int16, simulated on the
+    GPU), 128 x 128 x 256 volume, linear, no coherence factor. Decode on int8 tensor cores (hi/lo
+    byte split) checked bit-exact against the FWHT decode; analytic signal stored as FP32 and as
+    BF16, each compared with the FP64 oracle on 64 sampled rows; volumes from both storages."""
+    import torch
+    from cuda_ultrasound_toolkit_b200 import Plan, synth
+    from cuda_ultrasound_toolkit_b200.simulate import Simulator
+    from oracle import oracle as O
+    w = synth.CONFIGS["precision"]
+    rng = np.random.default_rng(seed)
+    cmap = rng.permutation(w.C).astype(np.int16)
+    scat = synth.phantom(rng, w.scatterers, 0, box_xy=w.box_xy, z_range=w.z_range)
+    raw, _ = Simulator(w.T, w.C, w.S).run(scat, cmap, seed)
+    bp = synth.make_params(w, channel_map=cmap)
+    p_tc, p_fw, p_bf = Plan(bp, decode_tc=True), Plan(bp), Plan(bp, decode_tc=True, iq_bf16=True)
+
+    def timed(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    dec_tc, dec_fw = p_tc.empty_decoded(), p_fw.empty_decoded()
+    tc_ms = timed(lambda: p_tc.decode(raw, out=dec_tc))
+    fw_ms = timed(lambda: p_fw.decode(raw, out=dec_fw))
+    exact = bool(torch.equal(dec_tc, dec_fw))
+    del dec_fw
+    iq32, iq16 = p_tc.empty_iq(), p_bf.empty_iq()
+    hil32_ms = timed(lambda: p_tc.hilbert(dec_tc, out=iq32))
+    hil16_ms = timed(lambda: p_bf.hilbert(dec_tc, out=iq16))
+    rows = np.sort(rng.choice(w.T * w.C, 64, replace=False))
+    d = dec_tc.view(w.T * w.C, w.S)[torch.from_numpy(rows).cuda()].double().cpu().numpy()
+    ref = O.hilbert(d.reshape(1, 64, w.S)).reshape(64, w.S)
+    g32 = iq32.view(w.T * w.C, w.S)[torch.from_numpy(rows).cuda()].cpu().numpy()
+    g16 = iq16.view(w.T * w.C, w.S, 2)[torch.from_numpy(rows).cuda()].float().cpu().numpy()
+    g16 = g16[..., 0] + 1j * g16[..., 1]
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))  # noqa: E731
+    vol32, vol16 = p_tc.empty_volume(), p_bf.empty_volume()
+    das32_ms = timed(lambda: p_tc.das(iq32, out=vol32), 2)
+    das16_ms = timed(lambda: p_bf.das(iq16, out=vol16), 2)
+    p_tc.check()
+    p_bf.check()
+    vol_rel = float(torch.linalg.vector_norm(vol16 - vol32) / torch.linalg.vector_norm(vol32))
+    dec_bytes = w.T * w.C * w.S * 6
+    return {"workload": "rca256 precision: 256 tx x 256 ch x 8192 samples -> 128x128x256, linear, no CF",
+            "decode_tc": {"ms": tc_ms, "bit_exact_vs_fwht": exact, "achieved_gbs": dec_bytes / tc_ms / 1e6},
+            "decode_fwht": {"ms": fw_ms, "achieved_gbs": dec_bytes / fw_ms / 1e6},
+            "analytic_signal": {"fp32": {"rel_l2_vs_fp64": rel(g32, ref), "hilbert_ms": hil32_ms},
+                                "bf16": {"rel_l2_vs_fp64": rel(g16, ref), "hilbert_ms": hil16_ms},
+                                "sample": "64 random rows of 65536, FP64 oracle Hilbert of the same decoded rows"},
+            "volume": {"das_ms_fp32_iq": das32_ms, "das_ms_bf16_iq": das16_ms,
+                       "bf16_vs_fp32_iq_rel_l2": vol_rel,
+                       "volumes_per_s_fp32_iq": 1e3 / (tc_ms + hil32_ms + das32_ms),
+                       "volumes_per_s_bf16_iq": 1e3 / (tc_ms + hil16_ms + das16_ms)}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -419,6 +486,7 @@ def main():
     ap.add_argument("--learned", type=int, default=16,
                     help="held-out volumes for the learned sparse-transmit path (0: skip)")
     ap.add_argument("--batched", type=int, default=64, help="frames of the batched mixed-size stream (0: skip)")
+    ap.add_argument("--precision", type=int, default=1, help="run the 256 x 256 x 8192 precision form (0: skip)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

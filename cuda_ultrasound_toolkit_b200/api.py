@@ -163,7 +163,8 @@ def beamform_f32(raw, bp, out=None):
 
 # ---- device-resident stages ----------------------------------------------------------------------
 class _Options(ctypes.Structure):
-    _fields_ = [("iq_bf16", ctypes.c_int), ("das_tile", ctypes.c_int), ("reserved", ctypes.c_int * 14)]
+    _fields_ = [("iq_bf16", ctypes.c_int), ("das_tile", ctypes.c_int), ("decode_tc", ctypes.c_int),
+                ("reserved", ctypes.c_int * 13)]
 
 
 def _stream_handle(stream):
@@ -177,10 +178,10 @@ class Plan:
     """cutb_plan over torch CUDA tensors. Stage calls are asynchronous on `stream`
     (default: the current torch stream)."""
 
-    def __init__(self, bp: CudaBeamformerParameters, iq_bf16=False, das_tile=0):
+    def __init__(self, bp: CudaBeamformerParameters, iq_bf16=False, das_tile=0, decode_tc=False):
         import torch  # noqa: F401  (device memory comes from torch)
         self.bp = bp.copy()
-        opts = _Options(int(iq_bf16), int(das_tile))
+        opts = _Options(int(iq_bf16), int(das_tile), int(decode_tc))
         self._h = lib().cutb_plan_create(ctypes.byref(self.bp), ctypes.byref(opts))
         _check(self._h, "cutb_plan_create")
         self.iq_bf16 = bool(iq_bf16)
@@ -269,7 +270,7 @@ class Batch:
         self._bps = (CudaBeamformerParameters * n)(*[bp.copy() for bp in params])
         opts = None
         if das_tiles is not None:
-            opts = (_Options * n)(*[_Options(0, int(t)) for t in das_tiles])
+            opts = (_Options * n)(*[_Options(0, int(t), 0) for t in das_tiles])
         self._h = lib().cutb_batch_create(self._bps, opts, n)
         _check(self._h, "cutb_batch_create")
         self.n = n

@@ -1,0 +1,208 @@
+// Convert + reorder + Hadamard/Walsh decode as an exact int8 tensor-core contraction.
+//
+// Upstream decodes with one FP32 GEMM, dec[t'][c][s] = fl32(1/T) * sum_t H[t'][t] * x[t][c][s]
+// (hadamard_decoder.cpp:49-78). Every raw sample is an int16, x = 256 * hi + lo with hi the
+// signed high byte and lo the unsigned low byte, so
+//     sum_t H[t'][t] x[t] = 256 * (H . x_hi)[t'] + (H . x_lo)[t']
+// and both products are int8 MMAs (tcgen05 kind::i8, int32 accumulation) with H in {-1, +1}.
+// |H . x_hi| <= 128 T and |H . x_lo| <= 255 T, so for T <= 256 the combination is exact in int32
+// and, scaled by fl32(1/T), bit-identical to the FWHT path and to upstream's FP32 GEMM.
+//
+// A CTA decodes one receive channel c over N samples: A = H (M = 128 output rows per tile, K =
+// transmits, K-major, rows beyond T zero) comes from a prebuilt canonical image by one bulk
+// copy; the threads load the int16 tile [T][N] of raw channel map[c] with 16-byte loads, split
+// it into a signed-high and an unsigned-low byte plane written in the MN-major operand layout
+// (16 samples x 8 transmits per core matrix), and one thread issues the MMAs: per 32 transmits
+// one for each plane into its own TMEM accumulator. The epilogue combines hi and lo, scales and
+// stores rows t' of [T][C][S].
+#include "common.cuh"
+#include "stages.h"
+#include "tc05.cuh"
+
+namespace cutb {
+namespace {
+
+using namespace tc;
+
+constexpr int kThreads = 128;
+
+// Canonical A image: M tile m, row r (t' = 128 m + r), transmit k at
+//   m * 128 * T + (r / 8) * (T / 16) * 128 + (k / 16) * 128 + (r % 8) * 16 + (k % 16).
+__host__ __device__ constexpr size_t a_offset(int T, int m, int r, int k)
+{
+    return (size_t)m * 128 * T + (size_t)(r / 8) * (T / 16) * 128 + (size_t)(k / 16) * 128 + (r % 8) * 16 + (k % 16);
+}
+
+template <int MT, int N>
+struct DecCfg {
+    static constexpr uint32_t kTmemCols = 2u * MT * N;  // hi and lo accumulators per M tile
+    static_assert(kTmemCols <= 256, "two CTAs per SM");
+    static constexpr uint32_t kLboB = (N / 16) * 128;    // stride of 8-transmit groups in a plane
+};
+
+template <int MT, int N, int OSTRIDE>
+__global__ void __launch_bounds__(kThreads, 2) decode_tc_kernel(const int16_t* __restrict__ raw,
+                                                                const int8_t* __restrict__ a_image, DecodeTcArgs a)
+{
+    using C = DecCfg<MT, N>;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ uint64_t a_full, mma_done;
+    __shared__ uint32_t tmem_base_s;
+    const int T = (int)a.T;
+    const uint32_t a_bytes = (uint32_t)MT * 128 * T;
+    uint8_t* A = smem;
+    uint8_t* Bhi = smem + a_bytes;
+    uint8_t* Blo = Bhi + (uint32_t)T * N;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int c = blockIdx.y;
+    const int s0 = blockIdx.x * N;
+    if (tid == 0) {
+        mbar_init(&a_full, 1);
+        mbar_init(&mma_done, 1);
+        fence_mbar_init();
+    }
+    if (warp == 0) {
+        tmem_alloc(&tmem_base_s, C::kTmemCols);
+        tmem_relinquish();
+    }
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = tmem_base_s;
+    if (tid == 0) {
+        mbar_arrive_expect_tx(&a_full, a_bytes);
+        bulk_load(A, a_image, a_bytes, &a_full);
+    }
+
+    // Raw tile -> signed-high and unsigned-low byte planes (MN-major: 16 samples x 8 transmits).
+    const int16_t* src = raw + (size_t)a.map[c] * a.R0;
+    constexpr int kVecPerRow = N / 8;
+    for (int v = tid; v < T * kVecPerRow; v += kThreads) {
+        const int t = v / kVecPerRow, j = v % kVecPerRow;
+        const int s = s0 + 8 * j;
+        uint4 x = make_uint4(0, 0, 0, 0);
+        if (s < (int)a.S) x = __ldcs(reinterpret_cast<const uint4*>(src + (size_t)t * a.S + s));
+        const uint32_t w[4] = {x.x, x.y, x.z, x.w};
+        uint32_t hi[2], lo[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            // bytes of samples 4h..4h+3: low bytes and high bytes of the four int16 values
+            const uint32_t p = w[2 * h], q = w[2 * h + 1];
+            lo[h] = __byte_perm(p, q, 0x6420);
+            hi[h] = __byte_perm(p, q, 0x7531);
+        }
+        const uint32_t off = (t / 8) * C::kLboB + ((8 * j) / 16) * 128 + (t % 8) * 16 + (8 * j) % 16;
+        *reinterpret_cast<uint2*>(Bhi + off) = make_uint2(hi[0], hi[1]);
+        *reinterpret_cast<uint2*>(Blo + off) = make_uint2(lo[0], lo[1]);
+    }
+    fence_proxy_async_shared();
+    __syncthreads();
+
+    int ok_local = 1;
+    if (tid == 0) {
+        if (!mbar_wait(&a_full, 0)) {
+            if (a.status) atomicOr(a.status, 2);
+            ok_local = 0;
+        } else {
+            fence_after_sync();
+            constexpr uint32_t id_hi = idesc_i8(128, N, true, true, false, true);
+            constexpr uint32_t id_lo = idesc_i8(128, N, true, false, false, true);
+            const uint32_t sa = saddr(A), shi = saddr(Bhi), slo = saddr(Blo);
+            const uint32_t sbo_a = (uint32_t)(T / 16) * 128;
+            for (int m = 0; m < MT; ++m)
+                for (int ks = 0; ks < T / 32; ++ks) {
+                    const uint64_t ad = smem_desc(sa + m * 128 * T + ks * 256, 128, sbo_a);
+                    const uint64_t bh = smem_desc(shi + ks * 4 * C::kLboB, C::kLboB, 128);
+                    const uint64_t bl = smem_desc(slo + ks * 4 * C::kLboB, C::kLboB, 128);
+                    mma_i8(tmem + (2 * m) * N, ad, bh, id_hi, ks > 0);
+                    mma_i8(tmem + (2 * m + 1) * N, ad, bl, id_lo, ks > 0);
+                }
+        }
+        mma_commit(&mma_done);
+    }
+    __syncwarp();
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(&mma_done, 0)) && __shfl_sync(0xffffffffu, ok_local, 0);
+    fence_after_sync();
+    if (!ok) {
+        if (lane == 0 && a.status) atomicOr(a.status, 2);
+    } else {
+        const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
+        for (int m = 0; m < MT; ++m) {
+            const int tp = m * 128 + 32 * warp + lane;  // output row
+#pragma unroll 1
+            for (int q = 0; q < N / 8; ++q) {
+                int h[8], l[8];
+                tmem_ld8_i32(lane_addr + (2 * m) * N + 8 * q, h);
+                tmem_ld8_i32(lane_addr + (2 * m + 1) * N + 8 * q, l);
+                tmem_wait_ld();
+                const int s = s0 + 8 * q;
+                if (tp >= T || s >= (int)a.S) continue;
+                float f[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) f[i] = __fmul_rn((float)(h[i] * 256 + l[i]), a.alpha);
+                float* o = a.out + (((size_t)tp * a.C + c) * a.S + s) * OSTRIDE;
+                if (OSTRIDE == 1) {
+                    reinterpret_cast<float4*>(o)[0] = make_float4(f[0], f[1], f[2], f[3]);
+                    reinterpret_cast<float4*>(o)[1] = make_float4(f[4], f[5], f[6], f[7]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 8; i += 2)
+                        reinterpret_cast<float4*>(o)[i / 2] = make_float4(f[i], 0.f, f[i + 1], 0.f);
+                }
+            }
+        }
+    }
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, C::kTmemCols);
+}
+
+template <int MT, int N, int OSTRIDE>
+bool launch_tc(const int16_t* raw, const int8_t* image, const DecodeTcArgs& a, cudaStream_t st)
+{
+    auto k = decode_tc_kernel<MT, N, OSTRIDE>;
+    const uint32_t used = (uint32_t)MT * 128 * a.T + 2u * a.T * N;
+    // at most two CTAs per SM, so that their TMEM (2 x 256 columns) always fits
+    const uint32_t smem = used > 80u * 1024 ? used : 80u * 1024;
+    CUTB_CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const dim3 grid((a.S + N - 1) / N, a.C);
+    k<<<grid, kThreads, smem, st>>>(raw, image, a);
+    CUTB_CUDA_OK(cudaGetLastError());
+    return true;
+}
+
+}  // namespace
+
+bool decode_tc_supported(uint32_t T, uint32_t S, uint64_t R0)
+{
+    return T >= 32 && T <= 256 && T % 32 == 0 && S % 8 == 0 && R0 % 8 == 0;
+}
+
+bool build_decode_tc_image(const int8_t* H, uint32_t T, std::vector<int8_t>& image)
+{
+    const int MT = T > 128 ? 2 : 1;
+    image.assign((size_t)MT * 128 * T, 0);
+    for (int m = 0; m < MT; ++m)
+        for (int r = 0; r < 128; ++r) {
+            const int tp = m * 128 + r;
+            if (tp >= (int)T) continue;
+            for (int k = 0; k < (int)T; ++k) image[a_offset((int)T, m, r, k)] = H[(size_t)tp * T + k];
+        }
+    return true;
+}
+
+bool launch_decode_tc(const DecodeTcArgs& a, const int8_t* image, const void* raw, unsigned out_stride,
+                      cudaStream_t st)
+{
+    CUTB_REQUIRE(decode_tc_supported(a.T, a.S, a.R0), CUTB_ERR_UNSUPPORTED,
+                 "Tensor-core decode needs 32..256 transmits in steps of 32 and 8-sample aligned rows.");
+    CUTB_REQUIRE(((uintptr_t)raw & 15) == 0 && ((uintptr_t)a.out & 15) == 0 && ((uintptr_t)image & 15) == 0,
+                 CUTB_ERR_INVALID_ARGUMENT, "Tensor-core decode needs 16-byte aligned buffers.");
+    const int16_t* r = (const int16_t*)raw;
+    if (a.T > 128)
+        return out_stride == 1 ? launch_tc<2, 64, 1>(r, image, a, st) : launch_tc<2, 64, 2>(r, image, a, st);
+    return out_stride == 1 ? launch_tc<1, 128, 1>(r, image, a, st) : launch_tc<1, 128, 2>(r, image, a, st);
+}
+
+}  // namespace cutb

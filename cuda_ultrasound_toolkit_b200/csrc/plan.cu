@@ -183,6 +183,21 @@ bool FrontEnd::set_filter(const float* taps, uint32_t ntaps)
     return true;
 }
 
+bool FrontEnd::enable_tc_decode(int* status)
+{
+    CUTB_REQUIRE(d_out_row != nullptr, CUTB_ERR_NOT_INITIALIZED, "Session not initialized.");
+    CUTB_REQUIRE(dec.encoding != NONE, CUTB_ERR_UNSUPPORTED, "Tensor-core decode needs a Hadamard or Walsh code.");
+    CUTB_REQUIRE(decode_tc_supported(T, S, R0), CUTB_ERR_UNSUPPORTED,
+                 "Tensor-core decode needs 32..256 transmits in steps of 32 and rows of 8-sample multiples "
+                 "(T = %u, S = %u, R0 = %u).", T, S, R0);
+    std::vector<int8_t> H((size_t)T * T), image;
+    if (!cutb_encoding_matrix(T, dec.encoding, (signed char*)H.data())) return false;
+    build_decode_tc_image(H.data(), T, image);
+    if (!upload(&d_tc_image, image.data(), image.size())) return false;
+    d_status = status;
+    return true;
+}
+
 bool FrontEnd::decode(const void* d_raw, int data_type, float* d_out, unsigned out_stride, cudaStream_t st)
 {
     CUTB_REQUIRE(d_out_row != nullptr, CUTB_ERR_NOT_INITIALIZED, "Session not initialized.");
@@ -191,6 +206,18 @@ bool FrontEnd::decode(const void* d_raw, int data_type, float* d_out, unsigned o
                  "Data converter: Unsupported input data type %d.", data_type);
     CUTB_REQUIRE(out_stride == 1 || out_stride == 2, CUTB_ERR_INVALID_ARGUMENT, "Output stride must be 1 or 2.");
     CUTB_REQUIRE(d_raw && d_out, CUTB_ERR_INVALID_ARGUMENT, "Null device buffer.");
+    if (d_tc_image && data_type == TYPE_I16) {
+        DecodeTcArgs a{};
+        a.R0 = R0;
+        a.S = S;
+        a.C = C;
+        a.T = T;
+        a.map = d_map;
+        a.alpha = dec.args.alpha;
+        a.out = d_out;
+        a.status = d_status;
+        return launch_decode_tc(a, d_tc_image, d_raw, out_stride, st);
+    }
     return launch_decode(dec, d_raw, data_type, d_out, out_stride, st);
 }
 
@@ -208,6 +235,8 @@ bool FrontEnd::hilbert(const float* d_in, unsigned in_stride, void* d_iq, bool b
 
 void FrontEnd::release()
 {
+    device_free(d_tc_image);
+    d_tc_image = nullptr;
     device_free(d_map);
     device_free(d_out_row);
     device_free(d_tables);
@@ -394,6 +423,7 @@ bool cutb_plan::build(const CudaBeamformerParameters& params, const cutb_options
     if (!alloc_bytes((void**)&d_status, sizeof(int))) return false;
     CUTB_CUDA_OK(cudaMemset(d_status, 0, sizeof(int)));
     das.status = d_status;
+    if (opt.decode_tc && !fe.enable_tc_decode(d_status)) return false;
     return true;
 }
 

@@ -26,6 +26,21 @@ struct DecodeSetup {
 };
 
 bool plan_decode_split(unsigned T, unsigned base, unsigned& R, unsigned& L);
+
+// Tensor-core (int8 hi/lo byte split) decode of int16 input (decode_tc.cu).
+struct DecodeTcArgs {
+    uint64_t R0;
+    uint32_t S, C, T;
+    const int16_t* map;
+    float alpha;
+    float* out;
+    int* status;
+};
+bool decode_tc_supported(uint32_t T, uint32_t S, uint64_t R0);
+// Canonical shared-memory image of the encoding matrix H (row-major T x T, +-1) for the kernel.
+bool build_decode_tc_image(const int8_t* H, uint32_t T, std::vector<int8_t>& image);
+bool launch_decode_tc(const DecodeTcArgs& a, const int8_t* image, const void* raw, unsigned out_stride,
+                      cudaStream_t st);
 bool launch_decode(const DecodeSetup& d, const void* raw, int data_type, float* out, unsigned out_stride,
                    cudaStream_t st);
 

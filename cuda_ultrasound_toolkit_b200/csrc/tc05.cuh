@@ -56,6 +56,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
     return true;
 }
 
+// Orders this thread's generic-proxy shared-memory writes before later async-proxy reads
+// (tensor-core operands written by threads, then read through descriptors).
+__device__ __forceinline__ void fence_proxy_async_shared()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 // ---- TMA ------------------------------------------------------------------------------------
 __device__ __forceinline__ void prefetch_tensormap(const CUtensorMap* map)
 {

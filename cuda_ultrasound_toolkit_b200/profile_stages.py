@@ -17,9 +17,10 @@ def main():
     ap.add_argument("--workload", default="full", choices=sorted(synth.CONFIGS))
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--bf16", action="store_true", help="store the analytic signal as bf16")
+    ap.add_argument("--decode-tc", action="store_true", help="decode on int8 tensor cores")
     args = ap.parse_args()
     raw, bp = synth.frame(args.workload)
-    plan = Plan(bp, iq_bf16=args.bf16)
+    plan = Plan(bp, iq_bf16=args.bf16, decode_tc=args.decode_tc)
     d_raw = torch.from_numpy(raw).cuda()
     vol, dec, iq = plan.empty_volume(), plan.empty_decoded(), plan.empty_iq()
     plan.beamform(d_raw, out=vol)

@@ -62,7 +62,9 @@ CUTB_API bool cutb_encoding_matrix(uint n, int ordering, signed char* out);
 typedef struct cutb_options {
     int iq_bf16;      /* 1: analytic signal stored as bf16 complex (halves DAS gather bytes) */
     int das_tile;     /* delay-and-sum tile: 0 = chosen from the grid, 1 = 4x8x32, 2 = 8x8x16 (HERCULES) */
-    int reserved[14];
+    int decode_tc;    /* 1: int16 decode on int8 tensor cores (hi/lo byte split, exact); needs 32..256
+                         transmits in steps of 32 and rows of 8-sample multiples */
+    int reserved[13];
 } cutb_options;
 
 typedef struct cutb_plan cutb_plan;
