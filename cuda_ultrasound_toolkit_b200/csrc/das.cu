@@ -452,6 +452,108 @@ __device__ __forceinline__ void row_pass(const DasArgs& a, const Smem<IQ, CUBIC_
     }
 }
 
+// ---- packed FP32x2 arithmetic (Blackwell add/sub/mul/fma.f32x2) ---------------------------
+typedef unsigned long long f2x;
+__device__ __forceinline__ f2x pk(float a, float b)
+{
+    f2x r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void upk(f2x v, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); }
+__device__ __forceinline__ f2x fma2(f2x a, f2x b, f2x c)
+{
+    f2x d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ f2x add2(f2x a, f2x b)
+{
+    f2x d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2x add2_rm(f2x a, f2x b)
+{
+    f2x d;
+    asm("add.rm.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2x sub2(f2x a, f2x b)
+{
+    f2x d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2x mul2(f2x a, f2x b)
+{
+    f2x d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ float rsqrt_approx(float x)
+{
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// row_pass for HERCULES, cubic, staged rows, no apodization, on packed FP32x2 instructions:
+// the delay arithmetic of voxel pairs (2p, 2p + 1) runs element-wise in one instruction each,
+// and every voxel's complex Horner evaluation and accumulation in (re, im) pairs. Element by
+// element the operations are those of row_pass: -(exdx + sq) negates the rounded sum exactly,
+// so d0^2 - (-delta) = d0^2 + delta. Only the coherence energy is kept as (re^2, im^2) partial
+// sums, added at the end.
+template <bool CF, class IQ>
+__device__ __forceinline__ void row_pass_packed(const Smem<IQ, true>& sm, const RowMeta* rows, int qi, float dxe,
+                                                float spm, f2x ww, const f2x (&sq2)[kVpt / 2],
+                                                const f2x (&txs2)[kVpt / 2], f2x (&tot2)[kVpt], f2x (&inc2)[kVpt])
+{
+    constexpr float kMagic = 8388608.f;
+    const RowMeta& m = rows[qi];
+    const float exdx = m.ex2 * dxe;
+    const f2x nexdx2 = pk(-exdx, -exdx);
+    const f2x d0sq2 = pk(m.d0sq, m.d0sq), nd02 = pk(-m.d0, -m.d0), td02 = pk(m.two_d0, m.two_d0);
+    const f2x base2 = pk(m.base, m.base), spm2 = pk(spm, spm), mhalf2 = pk(-0.5f, -0.5f);
+    const f2x magic2 = pk(kMagic, kMagic);
+    const float loc = m.loclamp, hic = m.hiclamp;
+    const float4* cA = sm.coefA[qi];
+    const float4* cB = sm.coefB[qi];
+#pragma unroll
+    for (int p = 0; p < kVpt / 2; ++p) {
+        const f2x nd = sub2(nexdx2, sq2[p]);  // -delta
+        const f2x D = sub2(d0sq2, nd);        // d0^2 + delta
+        float D0, D1;
+        upk(D, D0, D1);
+        const f2x r = pk(rsqrt_approx(D0), rsqrt_approx(D1));
+        const f2x e0 = fma2(D, r, nd02);
+        const f2x res = fma2(e0, add2(e0, td02), nd);
+        const f2x corr = fma2(mul2(mhalf2, r), res, e0);
+        const f2x idx = fma2(corr, spm2, add2(base2, txs2[p]));
+        float x0, x1;
+        upk(idx, x0, x1);
+        x0 = fminf(fmaxf(x0, loc), hic);
+        x1 = fminf(fmaxf(x1, loc), hic);
+        const f2x ic = pk(x0, x1);
+        const f2x f = add2_rm(ic, magic2);
+        float f0, f1;
+        upk(f, f0, f1);
+        const int i0 = __float_as_int(f0) - __float_as_int(kMagic);
+        const int i1 = __float_as_int(f1) - __float_as_int(kMagic);
+        float t0, t1;
+        upk(sub2(ic, sub2(f, magic2)), t0, t1);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int i = h ? i1 : i0;
+            const f2x tt = h ? pk(t1, t1) : pk(t0, t0);
+            const float4 A = cA[i], B = cB[i];
+            const f2x v = fma2(fma2(fma2(pk(B.z, B.w), tt, pk(B.x, B.y)), tt, pk(A.z, A.w)), tt, pk(A.x, A.y));
+            tot2[2 * p + h] = fma2(ww, v, tot2[2 * p + h]);
+            if (CF) inc2[2 * p + h] = fma2(v, v, inc2[2 * p + h]);
+        }
+    }
+}
+
 // Thread layout. HERCULES: lanes are 4 (x) x 8 (y) neighbours, whose delays differ by less
 // than a sample or two, so their shared-memory reads fall in distinct banks or broadcast;
 // warps and the kVpt registers of a thread run along z. FORCES (no y): lanes along x.
@@ -539,12 +641,20 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
 #pragma unroll
     for (int v = 0; v < kVpt; ++v) qz[v] = fmaf(two_cz, dz[v], fmaf(dxe, dxe, fmaf(dye, dye, dz[v] * dz[v])));
 
+    // HERCULES + cubic without apodization accumulates on packed FP32x2 (row_pass_packed).
+    constexpr bool PACKED = HERC && CUBIC && !APO;
     float2 total[kVpt];
     float inc[kVpt];
+    f2x tot2[PACKED ? kVpt : 1], inc2[PACKED ? kVpt : 1], txs2[PACKED ? kVpt / 2 : 1];
 #pragma unroll
     for (int v = 0; v < kVpt; ++v) {
         total[v] = make_float2(0.f, 0.f);
         inc[v] = 0.f;
+        if constexpr (PACKED) {
+            tot2[v] = 0ull;
+            inc2[v] = 0ull;
+            if (v % 2 == 0) txs2[v / 2] = pk(txs[v], txs[v + 1]);
+        }
     }
 
     const int nchunks = div_up(a.C, kRows);
@@ -596,7 +706,25 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
             }
         }
         const IQ* grow0 = iq + ((size_t)st.t * a.C + st.c0) * a.S;
-        if (all_staged) {
+        if constexpr (PACKED) {
+            f2x sq2[kVpt / 2];
+#pragma unroll
+            for (int p = 0; p < kVpt / 2; ++p) sq2[p] = pk(sq[2 * p], sq[2 * p + 1]);
+            const f2x ww = pk(st.sign, st.sign);
+            if (all_staged) {
+#pragma unroll 2
+                for (int qi = 0; qi < st.nq; ++qi)
+                    row_pass_packed<CF>(sm, rows, qi, dxe, a.spm, ww, sq2, txs2, tot2, inc2);
+            } else {
+                for (int qi = 0; qi < st.nq; ++qi) {
+                    if (rows[qi].len > 0)
+                        row_pass_packed<CF>(sm, rows, qi, dxe, a.spm, ww, sq2, txs2, tot2, inc2);
+                    else
+                        row_pass<SEQ, CUBIC, CF, APO, false>(a, sm, rows, b, qi, grow0 + (size_t)qi * a.S, st, dxe, sq,
+                                                             tsh, vzv, vx, a2, total, inc);
+                }
+            }
+        } else if (all_staged) {
 #pragma unroll 2
             for (int qi = 0; qi < st.nq; ++qi)
                 row_pass<SEQ, CUBIC, CF, APO, true>(a, sm, rows, b, qi, grow0, st, dxe, sq, tsh, vzv, vx, a2, total,
@@ -621,6 +749,17 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
         return;
     }
 
+    if constexpr (PACKED) {
+#pragma unroll
+        for (int v = 0; v < kVpt; ++v) {
+            float tx, ty, ix, iy;
+            upk(tot2[v], tx, ty);
+            upk(inc2[v], ix, iy);
+            total[v].x += tx;
+            total[v].y += ty;
+            inc[v] += ix + iy;
+        }
+    }
     if (x_idx >= a.X || y_idx >= a.Y) return;
 #pragma unroll
     for (int v = 0; v < kVpt; ++v) {
