@@ -904,7 +904,7 @@ bool derive_das(const CudaBeamformerParameters& bp, DasArgs& a)
                  CUTB_ERR_INVALID_ARGUMENT, "Invalid output points [%u, %u, %u].", bp.output_points[0],
                  bp.output_points[1], bp.output_points[2]);
     a.seq = bp.das_shader_id;
-    CUTB_REQUIRE(a.seq == HERCULES || a.seq == FORCES, CUTB_ERR_UNSUPPORTED,
+    CUTB_REQUIRE(a.seq == HERCULES || a.seq == FORCES || a.seq == RCA_TPW || a.seq == UFORCES, CUTB_ERR_UNSUPPORTED,
                  "Beamformer: Unsupported sequence ID %d.", (int)bp.das_shader_id);
 
     // beamformer.cu:25-36
@@ -947,6 +947,29 @@ bool derive_das(const CudaBeamformerParameters& bp, DasArgs& a)
         a.focus = bp.tx_orientation == bp.rx_orientation ? 1 : 2;
     } else {
         a.focus = bp.tx_orientation == bp.rx_orientation ? 3 : 4;
+    }
+
+    a.fc_over_fs = bp.center_frequency / bp.sampling_frequency;
+    if (a.seq == RCA_TPW || a.seq == UFORCES) {
+        // beamformer.cu:161-189, 416-468: no READI; TPW needs a plane focus, UFORCES the
+        // sparse-element table (and, for a defined transmit path, a focus in the x-z plane).
+        a.G = 1;
+        a.readi_row = 0;
+        a.apply_cf = 1;
+        a.use_apo = 1;
+        CUTB_REQUIRE(a.T <= MAX_ACQ_COUNT, CUTB_ERR_UNSUPPORTED, "At most %d transmits for this sequence.",
+                     MAX_ACQ_COUNT);
+        if (a.seq == RCA_TPW) {
+            CUTB_REQUIRE(a.focus == 1 || a.focus == 2, CUTB_ERR_UNSUPPORTED,
+                         "TPW beamforming requires a plane focus.");
+        } else {
+            CUTB_REQUIRE(bp.sparse_elements[0] != -1, CUTB_ERR_INVALID_ARGUMENT,
+                         "Beamformer: UFORCES requires sparse elements to be defined.");
+            CUTB_REQUIRE(a.focus == 3, CUTB_ERR_UNSUPPORTED,
+                         "UFORCES needs a focused transmit in the x-z plane (same row/column orientation).");
+            CUTB_REQUIRE(a.T >= 2, CUTB_ERR_INVALID_ARGUMENT, "UFORCES needs a flash plus at least one transmit.");
+        }
+        return true;
     }
 
     // READI sub-signals, beamformer.cu:56-61, 100-137, 235-251.
@@ -1066,6 +1089,12 @@ bool launch_das(const DasArgs& a, const void* iq, bool iq_bf16, void* volume, cu
     CUTB_REQUIRE(a.S % 4 == 0, CUTB_ERR_UNSUPPORTED,
                  "Delay-and-sum needs a sample count that is a multiple of 4 (got %d).", a.S);
     bool ok;
+    if (a.seq == RCA_TPW || a.seq == UFORCES) {
+        CUTB_REQUIRE(!a.tiles, CUTB_ERR_UNSUPPORTED, "Tile lists need HERCULES.");
+        const bool ok = launch_das_direct(a, iq, iq_bf16, volume, st);
+        if (ok && launches) ++*launches;
+        return ok;
+    }
     CUTB_REQUIRE(!a.tiles || (a.ntiles > 0 && a.ntiles <= (1 << 24)), CUTB_ERR_INVALID_ARGUMENT, "Bad tile list.");
     CUTB_REQUIRE(a.splits <= 1 || (a.tiles && !a.apply_cf && a.seq == HERCULES), CUTB_ERR_UNSUPPORTED,
                  "Split delay-and-sum needs a tile list, HERCULES and no coherence factor.");

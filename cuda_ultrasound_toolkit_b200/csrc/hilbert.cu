@@ -48,16 +48,14 @@ __device__ __forceinline__ void run_fft(cplx (&x)[16], uint32_t tau, const cplx*
     }
 }
 
-// Writes one component (PART 0 = real, 1 = imaginary) of output sample i.
-template <int PART>
-__device__ __forceinline__ void store_part(float2* out, uint64_t i, float v)
+// Writes output sample i (streaming: it is not read again by this kernel).
+__device__ __forceinline__ void store_iq(float2* out, uint64_t i, float re, float im)
 {
-    reinterpret_cast<float*>(out + i)[PART] = v;
+    __stcs(out + i, make_float2(re, im));
 }
-template <int PART>
-__device__ __forceinline__ void store_part(__nv_bfloat162* out, uint64_t i, float v)
+__device__ __forceinline__ void store_iq(__nv_bfloat162* out, uint64_t i, float re, float im)
 {
-    reinterpret_cast<__nv_bfloat16*>(out + i)[PART] = __float2bfloat16_rn(v);
+    out[i] = __floats2bfloat162_rn(re, im);
 }
 
 template <int LOGN>
@@ -98,26 +96,33 @@ hilbert_kernel(const float* __restrict__ in, OutT* __restrict__ out, HilbertArgs
         const float2 v = __ldg(t + k);
         return cplx{v.x, v.y};
     };
-    cplx w[16];
-    // IDFT(Z Ge) = Re(iq_a) + i Re(iq_b): written to the real parts.
-#pragma unroll
-    for (int m = 0; m < 16; ++m) w[m] = fft::cmul(z[m], weight(ge, tau + m * TPF));
-    run_fft<LOGN, +1>(w, tau, tw, sre, sim);
+    // IDFT(Z Ge) = Re(iq_a) + i Re(iq_b) and IDFT(Z Go) = Im(iq_a) + i Im(iq_b). Z Go waits in this
+    // thread's own slots of `keep` while the first inverse transform runs, then the first result
+    // waits there during the second, and every output sample is written once, whole. Only one
+    // 16-element array is live at a time.
+    float2* keep = reinterpret_cast<float2*>(smem + FPB * 2 * PN) + grp * N;
 #pragma unroll
     for (int m = 0; m < 16; ++m) {
-        const uint64_t n = tau + m * TPF;
-        if (has_a) store_part<0>(out, ra * N + n, w[m].x);
-        if (has_b) store_part<0>(out, rb * N + n, w[m].y);
+        const uint32_t k = tau + m * TPF;
+        const cplx o = fft::cmul(z[m], weight(go, k));
+        keep[k] = make_float2(o.x, o.y);
+        z[m] = fft::cmul(z[m], weight(ge, k));
     }
-    // IDFT(Z Go) = Im(iq_a) + i Im(iq_b): written to the imaginary parts.
+    run_fft<LOGN, +1>(z, tau, tw, sre, sim);
 #pragma unroll
-    for (int m = 0; m < 16; ++m) w[m] = fft::cmul(z[m], weight(go, tau + m * TPF));
-    run_fft<LOGN, +1>(w, tau, tw, sre, sim);
+    for (int m = 0; m < 16; ++m) {
+        const uint32_t k = tau + m * TPF;
+        const float2 o = keep[k];
+        keep[k] = make_float2(z[m].x, z[m].y);
+        z[m] = cplx{o.x, o.y};
+    }
+    run_fft<LOGN, +1>(z, tau, tw, sre, sim);
 #pragma unroll
     for (int m = 0; m < 16; ++m) {
         const uint64_t n = tau + m * TPF;
-        if (has_a) store_part<1>(out, ra * N + n, w[m].x);
-        if (has_b) store_part<1>(out, rb * N + n, w[m].y);
+        const float2 r = keep[n];
+        if (has_a) store_iq(out, ra * N + n, r.x, z[m].x);
+        if (has_b) store_iq(out, rb * N + n, r.y, z[m].y);
     }
 }
 
@@ -126,7 +131,7 @@ bool launch_hilbert_t(const float* in, void* out, const HilbertArgs& a, cudaStre
 {
     constexpr uint32_t N = 1u << LOGN;
     constexpr uint32_t FPB = hilbert_fft_per_block<LOGN>();
-    const size_t smem = (size_t)FPB * 2 * fft::spad_size(N) * sizeof(float);
+    const size_t smem = (size_t)FPB * (2 * fft::spad_size(N) * sizeof(float) + N * sizeof(float2));
     auto kern = hilbert_kernel<LOGN, OutT>;
     static bool configured = false;
     if (!configured) {

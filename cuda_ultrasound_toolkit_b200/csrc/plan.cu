@@ -413,6 +413,15 @@ bool cutb_plan::build(const CudaBeamformerParameters& params, const cutb_options
     CUTB_REQUIRE(opt.das_tile >= 0 && opt.das_tile <= 2, CUTB_ERR_INVALID_ARGUMENT, "Unknown tile id %d.",
                  opt.das_tile);
     das.tile = opt.das_tile;
+    if (das.seq == RCA_TPW) {  // beamformer.cu:439-443: angle of transmit t in foci[t][2], radians
+        std::vector<float> angles(das.T);
+        for (int t = 0; t < das.T; ++t) angles[t] = bp.foci[3 * t + 2];
+        if (!upload(&d_angles, angles.data(), angles.size())) return false;
+        das.angles = d_angles;
+    } else if (das.seq == UFORCES) {
+        if (!upload(&d_elems, bp.sparse_elements, (size_t)das.T)) return false;
+        das.elems = d_elems;
+    }
 
     const size_t esize = data_type == TYPE_I16 ? 2 : 4;
     raw_bytes = (size_t)bp.rf_raw_dim[0] * bp.rf_raw_dim[1] * esize;
@@ -442,4 +451,6 @@ cutb_plan::~cutb_plan()
     device_free(d_iq);
     device_free(d_status);
     device_free(d_tiles);
+    device_free(d_angles);
+    device_free(d_elems);
 }

@@ -49,6 +49,8 @@ struct cutb_plan {
     void* d_iq = nullptr;
     int* d_status = nullptr;   // device-side error word of the stage kernels
     int* d_tiles = nullptr;    // tile list of cutb_das_tiles
+    float* d_angles = nullptr; // RCA_TPW plane-wave angles
+    short* d_elems = nullptr;  // UFORCES transmit elements
     uint32_t tiles_capacity = 0;
     int launches = 0;
 

@@ -84,6 +84,9 @@ struct DasArgs {
     float cf_power;            // coherence exponent in [0, 1]
     float to_power;            // sine apodization exponent
     unsigned long long readi_row;  // bit g set: sub-signal g negated
+    const float* angles;       // RCA_TPW: device plane-wave angles (foci[t][2]), T entries
+    const short* elems;        // UFORCES: device transmit element indices (sparse_elements), T entries
+    float fc_over_fs;          // RCA_TPW: centre / sampling frequency (IQ rotation)
     int tile;                  // HERCULES tile: 0 chosen from the grid, 1 = 4 x 8 x 32, 2 = 8 x 8 x 16
     const int* tiles;          // optional device list of tile ids (z-major); null = every tile
     int ntiles;
@@ -118,6 +121,8 @@ void das_grid_tiles(const DasArgs& a, int counts[3]);
 // validation as the upstream dispatcher (beamformer.cu:17-197).
 bool derive_das(const CudaBeamformerParameters& bp, DasArgs& a);
 bool launch_das(const DasArgs& a, const void* iq, bool iq_bf16, void* volume, cudaStream_t st, int* launches);
+// Tilted-plane-wave and UFORCES delay-and-sum (das_direct.cu).
+bool launch_das_direct(const DasArgs& a, const void* iq, bool iq_bf16, void* volume, cudaStream_t st);
 // Tile shape (x, y, z voxels) the delay-and-sum kernel uses for these arguments.
 void das_tile_shape(const DasArgs& a, int shape[3]);
 

@@ -511,6 +511,83 @@ cd forces_voxel(const Geometry& g, const double* iq, double vx, double vz)
     return total * coherence(total, inc, g.cf_power);
 }
 
+/* UFORCES voxel (beamformer_kernels.cu:93-172): the FORCES geometry with transmit elements from
+ * the sparse-element table. Transmit row 0 is a discarded flash, so transmit t < T - 1 reads row
+ * t + 1; the first used transmit is scaled by 1/sqrt(128); receive element c sits at
+ * xdc_mins.x + pitch/2 + c*pitch and transmit t at xdc_mins.x + pitch/2 + (elem[t] - elem[0])*pitch
+ * (the focal point of beamformer_kernels.cu:114 plus the element offsets); the index is clamped
+ * to [0, S-2] (the tap below sample 0 reads as 0 here); only the receive Hann window applies and
+ * the incoherent sum takes the windowed values; CF always applied. */
+cd uforces_voxel(const Geometry& g, const double* iq, const short* elems, double vx, double vz)
+{
+    static const double kISqrt128 = (double)0.088388347648318f;
+    cd total = 0;
+    double inc = 0;
+    const double fx = (double)(float)(g.xmin_x + (float)g.px / 2.f);
+    for (unsigned t = 0; t + 1 < g.T; ++t) {
+        const double txx = fx + (double)(elems[t] - elems[0]) * g.px - vx;
+        const double tx = std::sqrt(txx * txx + vz * vz);
+        for (unsigned c = 0; c < g.C; ++c) {
+            const double rxx = g.xmin_x - vx + g.px / 2 + (double)c * g.px;
+            const double rx = std::sqrt(rxx * rxx + vz * vz);
+            double idx = (rx + tx) * g.spm + g.delay;
+            idx = std::min(std::max(idx, 0.0), (double)g.S - 2.0);
+            const double* row = iq + ((size_t)(t + 1) * g.C + c) * g.S * 2;
+            cd v = sample_row(row, g.S, idx < 1.0 ? 1.0 : idx, g.interpolate);
+            if (idx < 1.0) {  /* [0, 1): taps -1..2 around sample 0, the tap below 0 reads 0 */
+                auto P = [&](long k) -> cd { return (k >= 0 && k < (long)g.S) ? cd(row[2 * k], row[2 * k + 1]) : cd(0, 0); };
+                const double tt = idx;
+                if (!g.interpolate) {
+                    v = P(0) + tt * (P(1) - P(0));
+                } else {
+                    cd pm1 = 0, p0 = P(0), p1 = P(1), p2 = P(2);
+                    cd m0 = 0.5 * (p1 - pm1), m1 = 0.5 * (p2 - p0);
+                    double t2 = tt * tt, t3 = t2 * tt;
+                    v = (2 * t3 - 3 * t2 + 1) * p0 + (-2 * t3 + 3 * t2) * p1 + (t3 - 2 * t2 + tt) * m0 + (t3 - t2) * m1;
+                }
+            }
+            if (t == 0) v *= kISqrt128;
+            v *= hann_apo(std::fabs(rxx), vz, g.fn_rx);
+            total += v;
+            inc += std::norm(v);
+        }
+    }
+    return total * coherence(total, inc, g.cf_power);
+}
+
+/* Tilted-plane-wave voxel (beamformer_kernels.cu:490-550, angles from foci[t][2] as in
+ * beamformer.cu:439-443): receive element c at xdc_mins.x + pitch/2 + c*pitch, distance in the
+ * x-z plane; transmit path lat*sin(a) + z*cos(a) with lat = y for a YZ plane, x otherwise; the
+ * receive Hann window skips values below 0.1; every sample is rotated by
+ * exp(i 2 pi idx fc / fs) after the clamp to [1, S-2]; the incoherent sum takes the windowed
+ * values; CF always applied. */
+cd tpw_voxel(const Geometry& g, const double* iq, const float* angles, double fc_fs, double vx, double vy, double vz)
+{
+    cd total = 0;
+    double inc = 0;
+    const double lat = g.focus == 2 ? vy : vx;
+    for (unsigned c = 0; c < g.C; ++c) {
+        const double rxx = g.xmin_x - vx + g.px / 2 + (double)c * g.px;
+        const double rx = std::sqrt(rxx * rxx + vz * vz);
+        const double apo = hann_apo(std::fabs(rxx), vz, g.fn_rx);
+        if (apo < 0.1) continue;
+        for (unsigned t = 0; t < g.T; ++t) {
+            const double a = angles[t];
+            const double tx = lat * std::sin(a) + vz * std::cos(a);
+            double idx = (rx + tx) * g.spm + g.delay;
+            idx = std::min(std::max(idx, 1.0), (double)g.S - 2.0);
+            const double* row = iq + ((size_t)t * g.C + c) * g.S * 2;
+            cd v = sample_row(row, g.S, idx, g.interpolate);
+            const double ph = 2.0 * M_PI * idx * fc_fs;
+            v *= cd(std::cos(ph), std::sin(ph));
+            v *= apo;
+            total += v;
+            inc += std::norm(v);
+        }
+    }
+    return total * coherence(total, inc, g.cf_power);
+}
+
 } // namespace
 
 extern "C" {
@@ -527,14 +604,23 @@ int orc_das(const double* iq, const CudaBeamformerParameters* bp, const int64_t*
 {
     Geometry g;
     if (derive(*bp, g) != 0) return -1;
+    std::vector<float> angles;
+    std::vector<short> elems;
     if (g.seq == HERCULES) {
         if (g.focus != 2 && g.focus != 4) return -1;
         if (g.G > 32) return -1;
     } else if (g.seq == FORCES) {
         if (g.G > 1 && g.encoding != 1) return -1;
+    } else if (g.seq == RCA_TPW) {
+        if ((g.focus != 1 && g.focus != 2) || g.T > 256) return -1;
+        for (unsigned t = 0; t < g.T; ++t) angles.push_back(bp->foci[t * 3 + 2]);
+    } else if (g.seq == UFORCES) {
+        if (g.focus != 3 || g.T < 2 || g.T > 256 || bp->sparse_elements[0] == -1) return -1;
+        for (unsigned t = 0; t < g.T; ++t) elems.push_back(bp->sparse_elements[t]);
     } else {
         return -1;
     }
+    const double fc_fs = (double)bp->center_frequency / (double)bp->sampling_frequency;
     size_t total = voxels ? nvox : (size_t)g.X * g.Y * g.Z;
     parallel_for(total, nthreads, [&](size_t b, size_t e) {
         for (size_t k = b; k < e; ++k) {
@@ -543,7 +629,10 @@ int orc_das(const double* iq, const CudaBeamformerParameters* bp, const int64_t*
             double vx = g.vmin[0] + (double)x * g.res[0];
             double vy = g.vmin[1] + (double)y * g.res[1];
             double vz = g.vmin[2] + (double)z * g.res[2];
-            cd v = g.seq == HERCULES ? hercules_voxel(g, iq, vx, vy, vz) : forces_voxel(g, iq, vx, vz);
+            cd v = g.seq == HERCULES  ? hercules_voxel(g, iq, vx, vy, vz)
+                   : g.seq == FORCES  ? forces_voxel(g, iq, vx, vz)
+                   : g.seq == RCA_TPW ? tpw_voxel(g, iq, angles.data(), fc_fs, vx, vy, vz)
+                                      : uforces_voxel(g, iq, elems.data(), vx, vz);
             out[2 * k] = v.real();
             out[2 * k + 1] = v.imag();
         }

@@ -55,20 +55,40 @@ VOLUMES = [
     ("forces_tx_to_sin", dict(seq=SequenceId.FORCES, apo=ApoType.TX_TO_SIN)),
     ("forces_both_to_sin", dict(seq=SequenceId.FORCES, apo=ApoType.BOTH_TO_SIN, cf=0.3)),
     ("forces_readi", dict(seq=SequenceId.FORCES, readi=2, readi_id=1)),
+    # Tilted plane waves (angles in foci[t][2]): a YZ plane (transmit rows, receive columns) and
+    # an XZ plane (same orientation).
+    ("tpw_yz", dict(seq=SequenceId.RCA_TPW, angles=np.linspace(-0.15, 0.15, 8), fn_rx=1.0, cf=0.5)),
+    ("tpw_xz", dict(seq=SequenceId.RCA_TPW, angles=np.linspace(-0.1, 0.2, 8), same_orientation=True, cf=1.0)),
+    # UFORCES (focused, same orientation, sparse transmit elements). X * Y is a multiple of the
+    # upstream kernel's 128-thread block: its `> X * Y` guard writes one voxel past a slice otherwise.
+    ("uforces", dict(seq=SequenceId.UFORCES, same_orientation=True, focus_z=25e-3, elems=[0, 1, 3, 4, 6, 7, 9, 10],
+                     fn_rx=1.0, cf=0.5, X=16, Y=8)),
+    ("uforces_dense", dict(seq=SequenceId.UFORCES, same_orientation=True, focus_z=30e-3, elems=list(range(8)), cf=1.0,
+                           X=16, Y=8)),
 ]
 
 
 def volume_params(cmap, seq=SequenceId.HERCULES, cf=0.0, fn_rx=0.0, fn_tx=0.0, apo=ApoType.RX_HANN, readi=0,
-                  readi_id=0, decode=EncodingMatrix.HADAMARD, focus_z=math.inf, time_offset=0.0):
-    w = synth.Workload("golden", 8, 8, 512, 12, 6, 20, 0, cubic=True, cf=cf, encoding=decode,
+                  readi_id=0, decode=EncodingMatrix.HADAMARD, focus_z=math.inf, time_offset=0.0, angles=None,
+                  same_orientation=False, elems=None, X=12, Y=6):
+    w = synth.Workload("golden", 8, 8, 512, X, Y, 20, 0, cubic=True, cf=cf, encoding=decode,
                        box_xy=1.5e-3, z_range=(4e-3, 16e-3))
     bp = synth.make_params(w, channel_map=cmap)
+    if same_orientation:
+        bp.tx_orientation = bp.rx_orientation
+    if angles is not None:
+        for t, a in enumerate(angles):
+            bp.foci[3 * t + 2] = float(a)
+    if elems is not None:
+        for t, e in enumerate(elems):
+            bp.sparse_elements[t] = int(e)
     bp.das_shader_id = int(seq)
     bp.fn_rx, bp.fn_tx = fn_rx, fn_tx
     bp.apo_type = int(apo)
     bp.to_power = 2
     bp.readi_group_count, bp.readi_group_id = readi, readi_id
-    bp.foci[2] = focus_z
+    if angles is None:
+        bp.foci[2] = focus_z
     bp.time_offset = time_offset
     return bp
 

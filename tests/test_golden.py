@@ -50,7 +50,7 @@ def test_frontend_matches_upstream(orc):
 def test_volumes_match_upstream(orc):
     g = _load("volumes.npz")
     names = sorted(k[:-7] for k in g.files if k.endswith(".params"))
-    assert len(names) == 12
+    assert len(names) == 16
     for n in names:
         bp = _params(g[n + ".params"])
         vol, _, _ = orc.pipeline(g["raw"], bp)

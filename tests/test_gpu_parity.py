@@ -258,6 +258,46 @@ def test_das_tile_list_rejects_bad_ids(torch):
         plan.das_tiles(iq, [10 ** 6])
 
 
+TPW_UFORCES_CASES = [
+    dict(seq=SequenceId.RCA_TPW, angles=np.linspace(-0.2, 0.2, 8), fn_rx=1.0, cf=0.5),          # YZ plane
+    dict(seq=SequenceId.RCA_TPW, angles=np.linspace(-0.1, 0.3, 8), same=True, cf=1.0),           # XZ plane
+    dict(seq=SequenceId.RCA_TPW, angles=np.linspace(-0.1, 0.1, 8), same=True, cubic=False, cf=0.0),
+    dict(seq=SequenceId.UFORCES, elems=[0, 2, 3, 5, 6, 8, 9, 11], same=True, focus_z=20e-3, fn_rx=1.0, cf=0.5),
+    dict(seq=SequenceId.UFORCES, elems=list(range(8)), same=True, focus_z=30e-3, cf=1.0, cubic=False),
+    dict(seq=SequenceId.UFORCES, elems=list(range(8)), same=True, focus_z=30e-3, cf=0.3, z=(0.0, 30e-3)),  # clamp at 0
+]
+
+
+@pytest.mark.parametrize("case", TPW_UFORCES_CASES, ids=lambda c: f"{int(c['seq'])}-" + "-".join(
+    f"{k}" for k in c if k != "seq"))
+@pytest.mark.parametrize("bf16", [False, True])
+def test_das_tpw_uforces_vs_fp64(torch, orc, case, bf16):
+    case = dict(case)
+    angles, elems, same = case.pop("angles", None), case.pop("elems", None), case.pop("same", False)
+    bp = das_params(**case)
+    if same:
+        bp.tx_orientation = bp.rx_orientation
+    if angles is not None:
+        for t, a in enumerate(angles):
+            bp.foci[3 * t + 2] = float(a)
+    if elems is not None:
+        for t, e in enumerate(elems):
+            bp.sparse_elements[t] = int(e)
+    S, C, T = bp.dims
+    iq = analytic_rows(orc, T, C, S, seed=21 + len(str(case)))
+    plan = Plan(bp, iq_bf16=bf16)
+    if bf16:
+        d = torch.from_numpy(np.stack([iq.real, iq.imag], -1).astype(np.float32)).cuda().to(torch.bfloat16)
+    else:
+        d = torch.from_numpy(iq.astype(np.complex64)).cuda()
+    got = plan.das(d).cpu().numpy()
+    plan.check()
+    ref = orc.das(iq, bp)
+    assert rel_l2(got, ref) < (2e-2 if bf16 else TOL_DAS_APO)
+    if bp.das_shader_id == SequenceId.UFORCES or bp.tx_orientation == bp.rx_orientation:  # y-invariant
+        assert (got == got[:, :1, :]).all()
+
+
 def test_das_bf16_storage(torch, orc):
     bp = das_params(cf=1.0)
     S, C, T = bp.dims
