@@ -202,8 +202,11 @@ class Plan:
 
     # Allocation helpers -------------------------------------------------------------------------
     def empty_decoded(self, out_stride=1):
+        """Decoded rows: S samples, or the 2 S reals of the IQ pairs of a bandpass plan."""
         import torch
         S, C, T = self.bp.dims
+        if self.bp.sample_type == 1:  # SAMPLE_BANDPASS
+            S *= 2
         return torch.empty((T, C, S * out_stride), dtype=torch.float32, device="cuda")
 
     def empty_iq(self):

@@ -93,11 +93,12 @@ struct cutb_batch {
             cutb_plan* p = plans[found];
             CUTB_REQUIRE(p->das.seq == HERCULES, CUTB_ERR_UNSUPPORTED,
                          "Frame %d: batched beamforming supports HERCULES frames.", i);
-            CUTB_REQUIRE(p->fe.fft_ok, CUTB_ERR_UNSUPPORTED, "Frame %d: sample count not supported by the FFT.", i);
+            CUTB_REQUIRE(p->fe.fft_ok || p->fe.bandpass, CUTB_ERR_UNSUPPORTED,
+                         "Frame %d: sample count not supported by the FFT.", i);
             const size_t samples = (size_t)bp[i].dec_data_dim[0] * bp[i].dec_data_dim[1] * bp[i].dec_data_dim[2];
             float* d = nullptr;
             void* q = nullptr;
-            if (device_alloc((void**)&d, samples * 4) != cudaSuccess) {
+            if (device_alloc((void**)&d, p->decoded_bytes) != cudaSuccess) {
                 set_error(CUTB_ERR_ALLOCATION, "Batch frame %d: decoded buffer allocation failed.", i);
                 return false;
             }

@@ -198,6 +198,25 @@ bool FrontEnd::enable_tc_decode(int* status)
     return true;
 }
 
+bool FrontEnd::enable_bandpass(uint32_t S_complex, double fd_over_fs, const float* taps, uint32_t ntaps)
+{
+    CUTB_REQUIRE(d_out_row != nullptr, CUTB_ERR_NOT_INITIALIZED, "Session not initialized.");
+    CUTB_REQUIRE(S == 2 * S_complex, CUTB_ERR_INVALID_ARGUMENT, "Bandpass rows hold IQ pairs.");
+    CUTB_REQUIRE(std::isfinite(fd_over_fs), CUTB_ERR_INVALID_ARGUMENT, "Demodulation frequency must be finite.");
+    CUTB_REQUIRE(ntaps <= S_complex, CUTB_ERR_INVALID_ARGUMENT, "Filter longer (%u) than the row (%u).", ntaps,
+                 S_complex);
+    device_free(d_fir);
+    d_fir = nullptr;
+    if (ntaps && !upload(&d_fir, taps, ntaps)) return false;
+    bandpass = true;
+    demod_args.rows = (uint64_t)T * C;
+    demod_args.S = (int)S_complex;
+    demod_args.L = (int)ntaps;
+    demod_args.taps = d_fir;
+    demod_args.fd_over_fs = fd_over_fs;
+    return true;
+}
+
 bool FrontEnd::decode(const void* d_raw, int data_type, float* d_out, unsigned out_stride, cudaStream_t st)
 {
     CUTB_REQUIRE(d_out_row != nullptr, CUTB_ERR_NOT_INITIALIZED, "Session not initialized.");
@@ -224,6 +243,11 @@ bool FrontEnd::decode(const void* d_raw, int data_type, float* d_out, unsigned o
 bool FrontEnd::hilbert(const float* d_in, unsigned in_stride, void* d_iq, bool bf16, cudaStream_t st)
 {
     CUTB_REQUIRE(d_out_row != nullptr, CUTB_ERR_NOT_INITIALIZED, "Session not initialized.");
+    if (bandpass) {
+        CUTB_REQUIRE(in_stride == 1, CUTB_ERR_INVALID_ARGUMENT, "Bandpass rows are read packed.");
+        CUTB_REQUIRE(d_in && d_iq, CUTB_ERR_INVALID_ARGUMENT, "Null device buffer.");
+        return launch_demod_fir(demod_args, d_in, d_iq, bf16, st);
+    }
     CUTB_REQUIRE(fft_ok && d_tables != nullptr, CUTB_ERR_UNSUPPORTED,
                  "Sample count %u not supported by the FFT (powers of two 16..%u).", S, kMaxHilbertLength);
     CUTB_REQUIRE(in_stride == 1 || in_stride == 2, CUTB_ERR_INVALID_ARGUMENT, "Input stride must be 1 or 2.");
@@ -237,6 +261,9 @@ void FrontEnd::release()
 {
     device_free(d_tc_image);
     d_tc_image = nullptr;
+    device_free(d_fir);
+    d_fir = nullptr;
+    bandpass = false;
     device_free(d_map);
     device_free(d_out_row);
     device_free(d_tables);
@@ -394,21 +421,31 @@ bool cutb_plan::build(const CudaBeamformerParameters& params, const cutb_options
     bp = params;
     if (options) opt = *options;
     iq_bf16 = opt.iq_bf16 != 0;
-    // cuda_toolkit.cpp:153-182: only SAMPLE_NORMAL runs the RF front end.
-    CUTB_REQUIRE(bp.sample_type == SAMPLE_NORMAL, CUTB_ERR_UNSUPPORTED, "Unsupported sample type: %d",
-                 (int)bp.sample_type);
+    // cuda_toolkit.cpp:153-182 runs the RF front end for SAMPLE_NORMAL only; bandpass IQ pairs
+    // take the demodulation path of RfProcessor::convert_demod here (see bandpass.cu).
+    CUTB_REQUIRE(bp.sample_type == SAMPLE_NORMAL || bp.sample_type == SAMPLE_BANDPASS, CUTB_ERR_UNSUPPORTED,
+                 "Unsupported sample type: %d", (int)bp.sample_type);
+    const bool bandpass = bp.sample_type == SAMPLE_BANDPASS;
     data_type = bp.data_type;
     CUTB_REQUIRE(data_type == TYPE_I16 || data_type == TYPE_F32, CUTB_ERR_UNSUPPORTED,
                  "Data converter: Unsupported input data type %d.", data_type);
     CUTB_REQUIRE(bp.decode == NONE || bp.decode == HADAMARD || bp.decode == WALSH, CUTB_ERR_INVALID_ARGUMENT,
                  "Invalid decode value %d.", (int)bp.decode);
     const uint32_t raw_dims[2] = {bp.rf_raw_dim[0], bp.rf_raw_dim[1]};
-    const uint32_t dec_dims[3] = {bp.dec_data_dim[0], bp.dec_data_dim[1], bp.dec_data_dim[2]};
+    CUTB_REQUIRE(!bandpass || bp.dec_data_dim[0] <= (1u << 29), CUTB_ERR_INVALID_ARGUMENT, "Too many samples.");
+    const uint32_t dec_dims[3] = {bandpass ? 2 * bp.dec_data_dim[0] : bp.dec_data_dim[0], bp.dec_data_dim[1],
+                                  bp.dec_data_dim[2]};
     if (!fe.init(raw_dims, dec_dims, bp.decode)) return false;
     if (!fe.set_channel_mapping(bp.channel_mapping, MAX_CHANNEL_COUNT)) return false;
     CUTB_REQUIRE(bp.filter_length <= MAX_FILTER_LENGTH, CUTB_ERR_INVALID_ARGUMENT, "Filter length %u exceeds %d.",
                  bp.filter_length, MAX_FILTER_LENGTH);
-    if (!fe.set_filter(bp.rf_filter, bp.filter_length)) return false;
+    if (bandpass) {
+        if (!fe.enable_bandpass(bp.dec_data_dim[0], (double)bp.center_frequency / (double)bp.sampling_frequency,
+                                bp.rf_filter, bp.filter_length))
+            return false;
+    } else if (!fe.set_filter(bp.rf_filter, bp.filter_length)) {
+        return false;
+    }
     if (!derive_das(bp, das)) return false;
     CUTB_REQUIRE(opt.das_tile >= 0 && opt.das_tile <= 2, CUTB_ERR_INVALID_ARGUMENT, "Unknown tile id %d.",
                  opt.das_tile);
@@ -428,7 +465,7 @@ bool cutb_plan::build(const CudaBeamformerParameters& params, const cutb_options
     const size_t samples = (size_t)bp.dec_data_dim[0] * bp.dec_data_dim[1] * bp.dec_data_dim[2];
     iq_bytes = samples * (iq_bf16 ? 4 : 8);
     vol_bytes = (size_t)bp.output_points[0] * bp.output_points[1] * bp.output_points[2] * 8;
-    decoded_bytes = samples * sizeof(float);
+    decoded_bytes = samples * sizeof(float) * (bandpass ? 2 : 1);
     if (!alloc_bytes((void**)&d_status, sizeof(int))) return false;
     CUTB_CUDA_OK(cudaMemset(d_status, 0, sizeof(int)));
     das.status = d_status;

@@ -22,12 +22,17 @@ struct FrontEnd {
     bool map_set = false;
     bool fft_ok = false;      // S is a length the FFT kernel supports
     int8_t* d_tc_image = nullptr;  // canonical encoding matrix of the tensor-core decode (null: FWHT)
+    bool bandpass = false;         // SAMPLE_BANDPASS: decode 2 S raw samples per row, then demod + FIR
+    DemodArgs demod_args{};
+    float* d_fir = nullptr;
     int* d_status = nullptr;       // status word the tensor-core decode reports bounded waits in
 
     bool init(const uint32_t raw_dims[2], const uint32_t dec_dims[3], int encoding);
     bool set_channel_mapping(const int16_t* map, size_t count);
     bool set_filter(const float* taps, uint32_t ntaps);
     bool enable_tc_decode(int* status);
+    // Bandpass plans: IQ pairs of `S` complex samples, demodulated at fd / fs and filtered.
+    bool enable_bandpass(uint32_t S_complex, double fd_over_fs, const float* taps, uint32_t ntaps);
     bool decode(const void* d_raw, int data_type, float* d_out, unsigned out_stride, cudaStream_t st);
     bool hilbert(const float* d_in, unsigned in_stride, void* d_iq, bool bf16, cudaStream_t st);
     bool ready() const { return d_out_row != nullptr; }

@@ -44,6 +44,15 @@ bool launch_decode_tc(const DecodeTcArgs& a, const int8_t* image, const void* ra
 bool launch_decode(const DecodeSetup& d, const void* raw, int data_type, float* out, unsigned out_stride,
                    cudaStream_t st);
 
+// ---- bandpass IQ demodulation + time-domain filter (bandpass.cu) ----------------------------
+struct DemodArgs {
+    uint64_t rows;             // T * C rows of S complex samples (2 S decoded reals in)
+    int S, L;                  // complex samples per row, filter taps
+    const float* taps;         // device, L entries (null when L == 0)
+    double fd_over_fs;         // demodulation frequency / sampling frequency
+};
+bool launch_demod_fir(const DemodArgs& a, const float* in, void* out, bool bf16, cudaStream_t st);
+
 // ---- analytic signal (hilbert.cu) --------------------------------------------------------
 constexpr unsigned kMaxHilbertLength = 16384;
 

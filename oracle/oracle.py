@@ -107,3 +107,37 @@ def pipeline(raw, bp, voxels=None, threads=0):
     taps = np.ctypeslib.as_array(bp.rf_filter)[: int(bp.filter_length)].astype(np.float32)
     iq = hilbert(dec, taps if len(taps) else None, threads)
     return das(iq, bp, voxels, threads), iq, dec
+
+
+def convert_demod(raw, bp, taps=None):
+    """FP64 restatement of the bandpass front end (TEST INFRASTRUCTURE ONLY).
+
+    Every two raw samples of a transmit are an IQ pair (data_conversion_kernels.cuh:46-65). The
+    transmit decode is applied exactly to the raw pairs first (as decode_i16 / decode_f64 with
+    2 S samples per row), then z[s] = (x[2s] - i x[2s+1]) exp(-i 2 pi s fc / fs)
+    (data_conversion_kernels.cuh:14-20, with fc the parameter block's centre frequency), then the
+    time-domain filter of data_conversion_kernels.cuh:67-102: correlation with the reversed taps,
+    normalised by the number of taps inside the row. Returns complex [T][C][S]."""
+    S, C, T = bp.dims
+    sub = bp.copy()
+    sub.dec_data_dim[0] = 2 * S
+    sub.sample_type = 0
+    if np.asarray(raw).dtype == np.int16:
+        dec = decode_i16(raw, sub).astype(np.float64)
+    else:
+        dec = decode_f64(raw, sub)
+    z = dec[..., 0::2] - 1j * dec[..., 1::2]
+    r = float(bp.center_frequency) / float(bp.sampling_frequency)
+    s = np.arange(S)
+    z = z * np.exp(-2j * np.pi * np.mod(s * r, 1.0))
+    if taps is None or len(taps) == 0:
+        return z
+    h = np.asarray(taps, dtype=np.float64)
+    L, half = len(h), len(h) // 2
+    acc = np.zeros_like(z)
+    cnt = np.zeros(S)
+    for i in range(L):
+        lo, hi = max(0, half - i), min(S, S + half - i)
+        acc[..., lo:hi] += z[..., lo + i - half:hi + i - half] * h[L - 1 - i]
+        cnt[lo:hi] += 1
+    return acc / cnt

@@ -32,6 +32,9 @@ def lib():
         L.cuda_set_match_filter.argtypes = [ctypes.POINTER(ctypes.c_float), u]
         L.cuda_decode.argtypes = [ctypes.c_size_t, u]
         L.cuda_hilbert.argtypes = [u, u]
+        L.ref_convert_demod.argtypes = [vp, ctypes.c_int, u, u, u, u, u, vp, ctypes.c_float, ctypes.c_float, vp,
+                                        ctypes.c_int, vp]
+        L.ref_convert_demod.restype = ctypes.c_int
         for f in ("init_cuda_configuration", "register_cuda_buffers", "cuda_set_channel_mapping",
                   "cuda_set_match_filter", "cuda_decode", "cuda_hilbert"):
             getattr(L, f).restype = ctypes.c_bool
@@ -79,3 +82,21 @@ def decode_and_hilbert(raw, bp, taps=None):
     if not ok:
         raise RuntimeError("upstream front end failed")
     return dec.real.copy(), iq
+
+
+def convert_demod(raw, bp, demod_freq, sample_freq, taps=None):
+    """RfProcessor::convert_demod of the upstream CPU build: complex64 [T][C][S] (S complex samples)."""
+    S, C, T = bp.dims
+    raw = np.ascontiguousarray(raw)
+    from cuda_ultrasound_toolkit_b200.params import InputDataTypes
+    dtype = int(InputDataTypes.TYPE_I16 if raw.dtype == np.int16 else InputDataTypes.TYPE_F32)
+    cmap = np.zeros(256, np.int16)
+    cmap[:C] = np.ctypeslib.as_array(bp.channel_mapping)[:C]
+    t = np.zeros(0, np.float32) if taps is None else np.ascontiguousarray(taps, dtype=np.float32)
+    out = np.zeros((T, C, S), np.complex64)
+    rc = lib().ref_convert_demod(raw.ctypes.data, dtype, int(bp.rf_raw_dim[0]), int(bp.rf_raw_dim[1]), S, C, T,
+                                 cmap.ctypes.data, float(demod_freq), float(sample_freq), t.ctypes.data if len(t) else None,
+                                 len(t), out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("upstream convert_demod failed")
+    return out

@@ -8,8 +8,9 @@ that build seeded synthetic inputs through upstream's entry points and stores in
   encoding_matrices.npz  every supported encoding order (HADAMARD and WALSH), from
                          HadamardDecoder::generate_hadamard (hadamard_decoder.cpp:110-222)
   frontend.npz           cuda_decode + cuda_hilbert outputs (cuda_toolkit_ogl.cpp:192-273)
-  volumes.npz            beamform_i16_matlab volumes (cuda_toolkit_matlab.cpp:9-22) for HERCULES
-                         and FORCES parameter sets
+  volumes.npz            beamform_i16_matlab volumes (cuda_toolkit_matlab.cpp:9-22) for HERCULES,
+                         FORCES, TPW and UFORCES parameter sets
+  bandpass.npz           RfProcessor::convert_demod (rf_processor.cpp:225-246) on bandpass IQ pairs
 
 Run from the repository root (needs the upstream sources and a C++ compiler, no GPU):
   make -C oracle -f Makefile.ref REF=/path/to/upstream && python tests/golden/make_golden.py
@@ -130,7 +131,35 @@ def main():
         vols[f"{name}.params"] = np.frombuffer(bytes(bp), np.uint8)
         vols[f"{name}.volume"] = ref.beamform(raw, bp)
     np.savez_compressed(os.path.join(HERE, "volumes.npz"), **vols)
-    for f in ("encoding_matrices.npz", "frontend.npz", "volumes.npz"):
+
+    # Bandpass IQ pairs through upstream's RfProcessor::convert_demod (no upstream entry point
+    # calls it): int16 and f32 input, with and without the time-domain filter.
+    bpd = {}
+    for name, dtype, ntaps, seed in (("i16_nofilter", np.int16, 0, 11), ("i16_filter", np.int16, 16, 12),
+                                     ("f32_filter", np.float32, 9, 13)):
+        rng = np.random.default_rng(seed)
+        T, C, S, pad, extra = 8, 6, 256, 6, 2
+        w = synth.Workload(name, T, C, S, 8, 8, 8, 0, cubic=True, cf=0.0, encoding=EncodingMatrix.NONE)
+        cmap = rng.permutation(C + extra)[:C].astype(np.int16)
+        bp = synth.make_params(w, channel_map=cmap, raw_padding=pad + T * S)
+        bp.rf_raw_dim[1] = C + extra
+        bp.sample_type = 1
+        if dtype == np.int16:
+            raw = rng.integers(-32768, 32768, size=(C + extra, 2 * T * S + pad), dtype=np.int16)
+        else:
+            bp.data_type = 2
+            raw = rng.normal(0, 1000, size=(C + extra, 2 * T * S + pad)).astype(np.float32)
+        taps = synth.chirp_taps(ntaps) if ntaps else np.zeros(0, np.float32)
+        bp.filter_length = ntaps  # the parameter block carries the filter the plan applies
+        for i, v in enumerate(taps):
+            bp.rf_filter[i] = float(v)
+        bpd[f"{name}.raw"] = raw
+        bpd[f"{name}.params"] = np.frombuffer(bytes(bp), np.uint8)
+        bpd[f"{name}.taps"] = taps
+        bpd[f"{name}.iq"] = ref.convert_demod(raw, bp, bp.center_frequency, bp.sampling_frequency,
+                                              taps if ntaps else None)
+    np.savez_compressed(os.path.join(HERE, "bandpass.npz"), **bpd)
+    for f in ("encoding_matrices.npz", "frontend.npz", "volumes.npz", "bandpass.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")
 
 

@@ -87,3 +87,16 @@ def test_trained_weights_are_committed():
              (16, 16)]
     assert d["params"].size == sum(co * (27 * ci + 1) for ci, co in specs)
     assert np.all(np.isfinite(d["params"]))
+
+
+def test_bandpass_front_end_matches_upstream(orc):
+    """The oracle's bandpass demodulation + filter against upstream's RfProcessor::convert_demod."""
+    g = _load("bandpass.npz")
+    names = sorted(k[:-4] for k in g.files if k.endswith(".raw"))
+    assert len(names) == 3
+    for n in names:
+        bp = _params(g[n + ".params"])
+        taps = g[n + ".taps"]
+        got = orc.convert_demod(g[n + ".raw"], bp, taps if len(taps) else None)
+        want = g[n + ".iq"]
+        assert np.linalg.norm(got - want) / np.linalg.norm(want) < 1e-4, n

@@ -56,3 +56,15 @@ def test_volumes_match_upstream():
         assert err < TOL_VOLUME_UPSTREAM, (n, err)
         host = beamform_i16(raw, bp)                       # the MATLAB entry point, host spans
         assert np.array_equal(host, got), n
+
+
+def test_bandpass_front_end_matches_upstream():
+    import torch
+    g = np.load(os.path.join(GOLDEN, "bandpass.npz"))
+    for n in sorted(k[:-4] for k in g.files if k.endswith(".raw")):
+        bp = _params(g[n + ".params"])
+        plan = Plan(bp)
+        iq = plan.hilbert(plan.decode(torch.from_numpy(g[n + ".raw"]).cuda())).cpu().numpy()
+        plan.check()
+        want = g[n + ".iq"]
+        assert np.linalg.norm(iq - want) / np.linalg.norm(want) < 1e-4, n

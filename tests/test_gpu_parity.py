@@ -298,6 +298,49 @@ def test_das_tpw_uforces_vs_fp64(torch, orc, case, bf16):
         assert (got == got[:, :1, :]).all()
 
 
+BANDPASS_CASES = [
+    # (T, encoding, S, C, taps, f32 input)
+    (8, EncodingMatrix.NONE, 256, 6, 0, False), (16, EncodingMatrix.HADAMARD, 512, 4, 31, False),
+    (32, EncodingMatrix.WALSH, 128, 3, 8, True), (12, EncodingMatrix.HADAMARD, 300, 5, 64, False),
+]
+
+
+@pytest.mark.parametrize("T,enc,S,C,ntaps,f32", BANDPASS_CASES)
+def test_bandpass_front_end_vs_fp64(torch, orc, T, enc, S, C, ntaps, f32):
+    """Bandpass IQ pairs: exact transmit decode of the raw pairs, demodulation, time-domain filter."""
+    rng = np.random.default_rng(T * 7 + S)
+    R0, R1 = 2 * T * S + 4, C + 1
+    bp = base_params(S, C, T, R0=R0, R1=R1, decode=enc, cmap=rng.permutation(R1)[:C],
+                     data_type=InputDataTypes.TYPE_F32 if f32 else InputDataTypes.TYPE_I16)
+    bp.sample_type = 1
+    taps = synth.chirp_taps(ntaps) if ntaps else np.zeros(0, np.float32)
+    bp.filter_length = ntaps
+    for i, v in enumerate(taps):
+        bp.rf_filter[i] = float(v)
+    raw = rng.integers(-32768, 32768, size=(R1, R0), dtype=np.int16)
+    if f32:
+        raw = raw.astype(np.float32)
+    plan = Plan(bp)
+    dec = plan.decode(torch.from_numpy(raw).cuda())
+    iq = plan.hilbert(dec).cpu().numpy()
+    plan.check()
+    ref = orc.convert_demod(raw, bp, taps if ntaps else None)
+    assert rel_l2(iq, ref) < 2e-6
+
+
+def test_bandpass_pipeline_vs_oracle(torch, orc):
+    rng = np.random.default_rng(5)
+    T, C, S = 16, 8, 512
+    bp = das_params(S=S, C=C, T=T, z=(4e-3, 12e-3))
+    bp.sample_type = 1
+    bp.rf_raw_dim[0] = 2 * T * S
+    raw = rng.integers(-3000, 3000, size=(C, 2 * T * S), dtype=np.int16)
+    vol = Plan(bp).beamform(torch.from_numpy(raw).cuda()).cpu().numpy()
+    iq = orc.convert_demod(raw, bp)
+    vox = rng.choice(vol.size, 1024, replace=False)
+    assert rel_l2(vol.ravel()[vox], orc.das(iq, bp, vox)) < TOL_DAS_RANDOM
+
+
 def test_das_bf16_storage(torch, orc):
     bp = das_params(cf=1.0)
     S, C, T = bp.dims
@@ -382,7 +425,8 @@ def test_invalid_parameters_are_rejected(torch):
     bp = base_params(S, C, T, R0=T * S - 1); bad.append((bp, 1))               # rows shorter than T*S
     bp = base_params(S, C, 36); bad.append((bp, 2))                             # unsupported order
     bp = base_params(S, C, T); bp.channel_mapping[1] = 99; bad.append((bp, 1))  # map outside raw channels
-    bp = base_params(S, C, T); bp.sample_type = 1; bad.append((bp, 2))          # bandpass input
+    bp = base_params(S, C, T); bp.sample_type = 7; bad.append((bp, 2))          # unknown sample type
+    bp = base_params(S, C, T); bp.sample_type = 1; bad.append((bp, 1))          # bandpass: raw rows hold no IQ pairs
     bp = base_params(S, C, T); bp.data_type = 4; bad.append((bp, 2))            # u8 input
     bp = base_params(S, C, T); bp.das_shader_id = SequenceId.RCA_VLS; bad.append((bp, 2))
     bp = base_params(S, C, T); bp.rx_orientation = bp.tx_orientation; bad.append((bp, 2))  # XZ focus for HERCULES
