@@ -322,6 +322,11 @@ def run_ours(args, rank, world, local_rank):
             line["batched"] = batched_stream(args.batched)
         except Exception as exc:  # must not hide the plain pipeline's number
             line["batched"] = {"failed": str(exc)}
+    if args.motion and world == 1:
+        try:
+            line["motion"] = motion_section()
+        except Exception as exc:  # must not hide the plain pipeline's number
+            line["motion"] = {"failed": str(exc)}
     try:
         per_vol, sample = cpu_sample(frames[0][0], bp, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": 1.0 / per_vol, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
@@ -477,6 +482,108 @@ def precision_form(seed=3000):
                        "volumes_per_s_bf16_iq": 1e3 / (tc_ms + hil16_ms + das16_ms)}}
 
 
+def motion_section(reps=10, warmup=3):
+    """NCC block-matching motion detection: 16 B-mode-like frames of 512 x 512 (8-bit speckle,
+    translated up to 10 px), 32-pixel patches every 16 px (32 x 32 grid), +-16 px search (33 x 33
+    maps), every frame against frame 0. Ours: one fused launch over resident frames (device) and
+    cuda_toolkit::motion_detection with host frames (e2e); upstream's own GPU pipeline (its sources
+    built with NPP, oracle/_ref/libncc_ref.so) on the same host frames when it was built; the FP64
+    oracle on one frame pair as the CPU baseline. Inputs (16 MiB) fit in L2; the kernel is
+    compute-bound (FP32 correlation numerator)."""
+    import ctypes
+    import time
+    import torch
+    from cuda_ultrasound_toolkit_b200 import api
+    from cuda_ultrasound_toolkit_b200.params import NccMotionParameters
+    from cuda_ultrasound_toolkit_b200.synth import speckle_frames
+    from oracle import oracle as O
+    W = H = 512
+    F, P, sp, G, M = 16, 32, 16, 32, 16
+    rng = np.random.default_rng(77)
+    shifts = [(0.0, 0.0)] + [tuple(rng.uniform(-10, 10, 2)) for _ in range(F - 1)]
+    frames = speckle_frames(2024, W, H, shifts).astype(np.float32)
+    p = NccMotionParameters.make(frame_count=F, image_dims=(W, H), patch_size=P, motion_grid_spacing=sp,
+                                 motion_grid_dims=(G, G), search_margins=(M, M), abs_cor_threshold=0.3,
+                                 rel_cor_threshold=0.0, min_patch_variance=0.0, use_subpixel=True,
+                                 reference_frame=0, neighbour_compare=False)
+    vectors = (F - 1) * G * G
+    # algorithmic FLOPs of the correlation numerators (2 per template pixel per map position),
+    # window by window with the border clipping
+    flops = 0
+    for i in range(G):
+        for j in range(G):
+            t0, l0 = i * sp - P // 2, j * sp - P // 2
+            th = min(t0 + P - 1, H - 1) - max(t0, 0) + 1
+            tw = min(l0 + P - 1, W - 1) - max(l0, 0) + 1
+            sh = min(t0 + P - 1 + M, H - 1) - max(t0 - M, 0) + 1
+            sw = min(l0 + P - 1 + M, W - 1) - max(l0 - M, 0) + 1
+            flops += 2 * tw * th * (sw - tw + 1) * (sh - th + 1)
+    flops *= F - 1
+    d_frames = torch.from_numpy(frames).cuda()
+    d_maps = torch.empty((F, G, G, 4), dtype=torch.float32, device="cuda")
+    for _ in range(warmup):
+        api.motion_detection_device(d_frames, p, out=d_maps)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        api.motion_detection_device(d_frames, p, out=d_maps)
+    b.record()
+    torch.cuda.synchronize()
+    dev_ms = a.elapsed_time(b) / reps
+    ours = d_maps.cpu().numpy()
+    host_maps = np.empty_like(ours)
+    api.motion_detection(frames, p, out=host_maps)
+    t = time.perf_counter()
+    for _ in range(reps):
+        api.motion_detection(frames, p, out=host_maps)
+    e2e_ms = (time.perf_counter() - t) / reps * 1e3
+    fp32 = api.calibrate_fp32()
+    out = {"workload": f"{F} frames {W}x{H}, patch {P}, grid {G}x{G} every {sp} px, margins {M} "
+                       f"({2 * M + 1}x{2 * M + 1} maps), reference frame 0",
+           "vectors": vectors, "device_ms": dev_ms, "vectors_per_s": vectors / dev_ms * 1e3,
+           "e2e": {"ms": e2e_ms, "vectors_per_s": vectors / e2e_ms * 1e3, "h2d_bytes": frames.nbytes,
+                   "d2h_bytes": ours.nbytes, "api": "cuda_toolkit::motion_detection (host spans)"},
+           "roofline": {"bound": "fp32", "achieved_tflops": flops / dev_ms / 1e9, "peak_tflops": fp32,
+                        "frac": flops / dev_ms / 1e9 / fp32, "flops_per_launch": flops,
+                        "peak_source": "measured FP32 FMA probe (cutb_calibrate_fp32) on this GPU"},
+           "gpu_launches_per_call": 2, "host_equals_device": bool(np.array_equal(ours, host_maps))}
+    ref_lib = os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle", "_ref", "libncc_ref.so")
+    if os.path.exists(ref_lib):
+        # upstream's own pipeline (NPP + CUB kernels, three launches per grid point); it prints
+        # progress on stdout, which is silenced around the call
+        L = ctypes.CDLL(ref_lib)
+        fp = ctypes.POINTER(ctypes.c_float)
+        L.ref_motion_detection.argtypes = [fp, ctypes.POINTER(NccMotionParameters), fp]
+        ref_maps = np.zeros_like(ours)
+        sys.stdout.flush()
+        saved = os.dup(1)
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        try:
+            os.dup2(devnull, 1)
+            L.ref_motion_detection(frames.ctypes.data_as(fp), ctypes.byref(p), ref_maps.ctypes.data_as(fp))
+            t = time.perf_counter()
+            rc = L.ref_motion_detection(frames.ctypes.data_as(fp), ctypes.byref(p), ref_maps.ctypes.data_as(fp))
+            ref_ms = (time.perf_counter() - t) * 1e3
+        finally:
+            os.dup2(saved, 1)
+            os.close(saved)
+            os.close(devnull)
+        d = np.abs(ours - ref_maps)
+        out["upstream_gpu"] = {"ms": ref_ms, "vectors_per_s": vectors / ref_ms * 1e3, "rc": int(rc),
+                               "kind": "upstream image_processor.cpp + block_match_kernels.cu on NPP, host frames",
+                               "max_abs_diff_peak": float(d[..., 2:].max()),
+                               "max_abs_diff_offset": float(d[..., :2].max()),
+                               "same_accept_reject": bool(((ours[..., 2] > 0) == (ref_maps[..., 2] > 0)).all())}
+    t = time.perf_counter()
+    sub = NccMotionParameters.make(**{**p.as_dict(), "frame_count": 2})
+    O.motion_detection(frames[:2], sub, threads=os.cpu_count() or 1)
+    cpu_s = time.perf_counter() - t
+    out["cpu_baseline"] = {"vectors_per_s": G * G / cpu_s, "cores": os.cpu_count() or 1, "kind": "port",
+                           "sample": f"FP64 oracle, frames 0-1 ({G * G} vectors)"}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -487,6 +594,7 @@ def main():
                     help="held-out volumes for the learned sparse-transmit path (0: skip)")
     ap.add_argument("--batched", type=int, default=64, help="frames of the batched mixed-size stream (0: skip)")
     ap.add_argument("--precision", type=int, default=1, help="run the 256 x 256 x 8192 precision form (0: skip)")
+    ap.add_argument("--motion", type=int, default=1, help="run the NCC motion-detection section (0: skip)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

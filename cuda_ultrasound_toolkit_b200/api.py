@@ -11,13 +11,17 @@ missing or unloadable library raises):
   cutb_beamform) on torch CUDA tensors and the current torch stream.
 * ``RfSession``: the buffer-registry front end (init_cuda_configuration ... cuda_hilbert;
   upstream cuda_toolkit_ogl.cpp:105-273), with device tensors standing in for GL buffers.
+* ``motion_detection`` / ``corr_images`` (host arrays, cuda_toolkit::motion_detection and
+  ::corr_images, cuda_toolkit.cpp:201-329), their MATLAB forms ``motion_detect_f32`` /
+  ``corr_images_f32`` and the device forms ``motion_detection_device`` / ``corr_images_device``.
 """
 import ctypes
 import os
 
 import numpy as np
 
-from .params import CudaBeamformerParameters, InputDataTypes, MAX_CHANNEL_COUNT
+from .params import CorrImagesParameters, CudaBeamformerParameters, InputDataTypes, MAX_CHANNEL_COUNT, \
+    NccMotionParameters
 
 _LIB_NAME = "libcuda_toolkit_b200.so"
 _lib = None
@@ -84,6 +88,10 @@ def lib():
         "cuda_register_device_buffer": ([u, vp, sz], b),
         "beamform_i16_matlab": ([vp, CudaBeamformerParameters, vp], None),
         "beamform_f32_matlab": ([vp, CudaBeamformerParameters, vp], None),
+        "motion_detect_f32_matlab": ([vp, NccMotionParameters, vp], None),
+        "corr_images_f32_matlab": ([vp, vp, CorrImagesParameters, vp], None),
+        "cutb_motion_detection": ([vp, ctypes.POINTER(NccMotionParameters), vp, vp], b),
+        "cutb_corr_images": ([vp, vp, ctypes.POINTER(u), ctypes.POINTER(u), vp, vp], b),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -95,6 +103,16 @@ def lib():
     cxx.argtypes = [vp, sz, vp, sz, P]
     cxx.restype = b
     L.cxx_beamform = cxx
+    # cuda_toolkit::motion_detection(span<const u8>, span<u8>, const NccMotionParameters&) and
+    # cuda_toolkit::corr_images(span<const float>, span<const float>, span<float>, const uint*, const uint*)
+    mot = getattr(L, "_ZN12cuda_toolkit16motion_detectionESt4spanIKhLm18446744073709551615EES0_IhLm18446744073709551615EERK19NccMotionParameters")
+    mot.argtypes = [vp, sz, vp, sz, ctypes.POINTER(NccMotionParameters)]
+    mot.restype = b
+    L.cxx_motion_detection = mot
+    cor = getattr(L, "_ZN12cuda_toolkit11corr_imagesESt4spanIKfLm18446744073709551615EES2_S0_IfLm18446744073709551615EEPKjS5_")
+    cor.argtypes = [vp, sz, vp, sz, vp, sz, ctypes.POINTER(u), ctypes.POINTER(u)]
+    cor.restype = b
+    L.cxx_corr_images = cor
     _lib = L
     return L
 
@@ -158,6 +176,97 @@ def beamform_f32(raw, bp, out=None):
     code, msg = last_error()
     if code:
         raise CutbError("beamform_f32_matlab", code, msg)
+    return out
+
+
+# ---- image correlation and motion detection ------------------------------------------------------
+def _maps_shape(params):
+    return (int(params.frame_count), int(params.motion_grid_dims[1]), int(params.motion_grid_dims[0]), 4)
+
+
+def _corr_shape(template, source):
+    (th, tw), (sh, sw) = template.shape, source.shape
+    return (max(sh - th + 1, 0), max(sw - tw + 1, 0))
+
+
+def motion_detection(frames, params: NccMotionParameters, out=None):
+    """cuda_toolkit::motion_detection on host frames [F][H][W] (float32); returns the motion maps
+    [F][grid y][grid x][dx, dy, peak, no-shift peak]."""
+    frames = np.ascontiguousarray(frames, dtype=np.float32)
+    if out is None:
+        out = np.empty(_maps_shape(params), dtype=np.float32)
+    _check(lib().cxx_motion_detection(frames.ctypes.data, frames.nbytes, out.ctypes.data, out.nbytes,
+                                      ctypes.byref(params)), "cuda_toolkit::motion_detection")
+    return out
+
+
+def motion_detect_f32(frames, params: NccMotionParameters, out=None):
+    """motion_detect_f32_matlab (errors are only logged upstream; here they raise)."""
+    frames = np.ascontiguousarray(frames, dtype=np.float32)
+    if out is None:
+        out = np.empty(_maps_shape(params), dtype=np.float32)
+    lib().cutb_clear_error()
+    lib().motion_detect_f32_matlab(frames.ctypes.data, params, out.ctypes.data)
+    code, msg = last_error()
+    if code:
+        raise CutbError("motion_detect_f32_matlab", code, msg)
+    return out
+
+
+def corr_images(template, source, out=None, dims=None):
+    """cuda_toolkit::corr_images on host images [H][W]; returns the valid correlation map.
+    ``dims`` = ((tw, th), (sw, sh)) overrides the sizes passed (spans keep the arrays' sizes)."""
+    t = np.ascontiguousarray(template, dtype=np.float32)
+    s = np.ascontiguousarray(source, dtype=np.float32)
+    (tw, th), (sw, sh) = dims if dims is not None else ((t.shape[1], t.shape[0]), (s.shape[1], s.shape[0]))
+    if out is None:
+        out = np.empty((max(sh - th + 1, 0), max(sw - tw + 1, 0)), dtype=np.float32)
+    td = (ctypes.c_uint * 2)(tw, th)
+    sd = (ctypes.c_uint * 2)(sw, sh)
+    _check(lib().cxx_corr_images(t.ctypes.data, t.size, s.ctypes.data, s.size, out.ctypes.data, out.size, td, sd),
+           "cuda_toolkit::corr_images")
+    return out
+
+
+def corr_images_f32(template, source, out=None):
+    """corr_images_f32_matlab (errors raise here)."""
+    t = np.ascontiguousarray(template, dtype=np.float32)
+    s = np.ascontiguousarray(source, dtype=np.float32)
+    p = CorrImagesParameters()
+    p.template_dims[0], p.template_dims[1] = t.shape[1], t.shape[0]
+    p.source_dims[0], p.source_dims[1] = s.shape[1], s.shape[0]
+    if out is None:
+        out = np.empty(_corr_shape(t, s), dtype=np.float32)
+    lib().cutb_clear_error()
+    lib().corr_images_f32_matlab(t.ctypes.data, s.ctypes.data, p, out.ctypes.data)
+    code, msg = last_error()
+    if code:
+        raise CutbError("corr_images_f32_matlab", code, msg)
+    return out
+
+
+def motion_detection_device(frames, params: NccMotionParameters, out=None, stream=None):
+    """cutb_motion_detection on a CUDA float32 tensor [F][H][W]; asynchronous on `stream`."""
+    import torch
+    assert frames.is_cuda and frames.dtype == torch.float32 and frames.is_contiguous()
+    if out is None:
+        out = torch.empty(_maps_shape(params), dtype=torch.float32, device=frames.device)
+    _check(lib().cutb_motion_detection(frames.data_ptr(), ctypes.byref(params), out.data_ptr(),
+                                       _stream_handle(stream)), "cutb_motion_detection")
+    return out
+
+
+def corr_images_device(template, source, out=None, stream=None):
+    """cutb_corr_images on CUDA float32 tensors [H][W]; asynchronous on `stream`."""
+    import torch
+    assert template.is_cuda and source.is_cuda and template.dtype == source.dtype == torch.float32
+    template, source = template.contiguous(), source.contiguous()
+    if out is None:
+        out = torch.empty(_corr_shape(template, source), dtype=torch.float32, device=source.device)
+    td = (ctypes.c_uint * 2)(template.shape[1], template.shape[0])
+    sd = (ctypes.c_uint * 2)(source.shape[1], source.shape[0])
+    _check(lib().cutb_corr_images(template.data_ptr(), source.data_ptr(), td, sd, out.data_ptr(),
+                                  _stream_handle(stream)), "cutb_corr_images")
     return out
 
 

@@ -1,5 +1,6 @@
-// Upstream-compatible entry points: cuda_toolkit::beamform, the MATLAB wrappers and the
-// buffer-registry C ABI (include/cuda_toolkit.hpp, cuda_toolkit_matlab.h, cuda_toolkit_ogl.h).
+// Upstream-compatible entry points: cuda_toolkit::beamform, motion_detection and corr_images, the
+// MATLAB wrappers and the buffer-registry C ABI (include/cuda_toolkit.hpp, cuda_toolkit_matlab.h,
+// cuda_toolkit_ogl.h).
 //
 // Mirrors the upstream glue (cuda_toolkit/src/api/cuda_toolkit.cpp:109-199,
 // cuda_toolkit_matlab.cpp:9-37, cuda_toolkit_ogl.cpp:105-273): process-global cached
@@ -17,6 +18,7 @@
 #include "../../include/cuda_toolkit.hpp"
 #include "../../include/cuda_toolkit_matlab.h"
 #include "../../include/cuda_toolkit_ogl.h"
+#include "../../include/cuda_toolkit_b200_motion.h"
 #include "plan.h"
 
 using namespace cutb;
@@ -146,17 +148,85 @@ bool cuda_toolkit::beamform(std::span<const uint8_t> input_data, std::span<uint8
     return beamform_impl(input_data.data(), input_data.size(), output_data.data(), output_data.size(), bp);
 }
 
-bool cuda_toolkit::motion_detection(std::span<const uint8_t>, std::span<uint8_t>, const NccMotionParameters&)
+namespace {
+
+// Device copies of the host spans of the image entry points, kept between calls.
+struct ImageBuffers {
+    void* ptr[3] = {nullptr, nullptr, nullptr};
+    size_t bytes[3] = {0, 0, 0};
+    bool ensure(int i, size_t need)
+    {
+        if (bytes[i] >= need && ptr[i]) return true;
+        device_free(ptr[i]);
+        ptr[i] = nullptr;
+        bytes[i] = 0;
+        const cudaError_t e = device_alloc(&ptr[i], need ? need : 16);
+        CUTB_REQUIRE(e == cudaSuccess, CUTB_ERR_ALLOCATION, "Image buffer allocation of %zu bytes failed: %s", need,
+                     cudaGetErrorString(e));
+        bytes[i] = need;
+        return true;
+    }
+    ~ImageBuffers()
+    {
+        for (void* p : ptr) device_free(p);
+    }
+};
+
+ImageBuffers& image_buffers()
 {
-    set_error(CUTB_ERR_UNSUPPORTED, "motion_detection is not part of the RF -> volume library.");
-    return false;
+    static ImageBuffers b;
+    return b;
 }
 
-bool cuda_toolkit::corr_images(std::span<const float>, std::span<const float>, std::span<float>, const uint*,
-                               const uint*)
+}  // namespace
+
+// cuda_toolkit.cpp:201-238: frames copied to the device, one block-matching pass, maps copied back.
+bool cuda_toolkit::motion_detection(std::span<const uint8_t> images, std::span<uint8_t> motion_maps,
+                                    const NccMotionParameters& params)
 {
-    set_error(CUTB_ERR_UNSUPPORTED, "corr_images is not part of the RF -> volume library.");
-    return false;
+    std::lock_guard<std::mutex> lock(api_mutex());
+    const size_t in = sizeof(float) * (size_t)params.image_dims[0] * params.image_dims[1] * params.frame_count;
+    const size_t out =
+        4 * sizeof(float) * (size_t)params.motion_grid_dims[0] * params.motion_grid_dims[1] * params.frame_count;
+    CUTB_REQUIRE(images.data() && images.size() >= in, CUTB_ERR_INVALID_ARGUMENT,
+                 "Input image span holds %zu bytes, %u frames of %u x %u floats need %zu.", images.size(),
+                 params.frame_count, params.image_dims[0], params.image_dims[1], in);
+    CUTB_REQUIRE(motion_maps.data() && motion_maps.size() >= out, CUTB_ERR_INVALID_ARGUMENT,
+                 "Motion map span holds %zu bytes, the maps need %zu.", motion_maps.size(), out);
+    CUTB_CUDA_OK(cudaSetDevice(0));
+    auto& b = image_buffers();
+    if (!b.ensure(0, in) || !b.ensure(1, out)) return false;
+    CUTB_CUDA_OK(cudaMemcpy(b.ptr[0], images.data(), in, cudaMemcpyHostToDevice));
+    if (!cutb_motion_detection((const float*)b.ptr[0], &params, (float*)b.ptr[1], nullptr)) return false;
+    CUTB_CUDA_OK(cudaMemcpy(motion_maps.data(), b.ptr[1], out, cudaMemcpyDeviceToHost));
+    return true;
+}
+
+// cuda_toolkit.cpp:240-329, with upstream's argument checks and messages.
+bool cuda_toolkit::corr_images(std::span<const float> template_image, std::span<const float> source_image,
+                               std::span<float> corr_map, const uint template_dims[2], const uint source_dims[2])
+{
+    std::lock_guard<std::mutex> lock(api_mutex());
+    CUTB_REQUIRE(template_dims && source_dims, CUTB_ERR_INVALID_ARGUMENT, "Invalid image dimensions for corr_images.");
+    const size_t tw = template_dims[0], th = template_dims[1], sw = source_dims[0], sh = source_dims[1];
+    CUTB_REQUIRE(tw && th && sw && sh, CUTB_ERR_INVALID_ARGUMENT, "Invalid image dimensions for corr_images.");
+    CUTB_REQUIRE(tw <= sw && th <= sh, CUTB_ERR_INVALID_ARGUMENT,
+                 "Template dimensions must be <= source dimensions for corr_images.");
+    const size_t nt = tw * th, ns = sw * sh, nc = (sw - tw + 1) * (sh - th + 1);
+    CUTB_REQUIRE(template_image.size() >= nt && source_image.size() >= ns, CUTB_ERR_INVALID_ARGUMENT,
+                 "Input image spans are smaller than the provided dimensions for corr_images.");
+    CUTB_REQUIRE(corr_map.size() >= nc, CUTB_ERR_INVALID_ARGUMENT, "Output corr_map span is too small for corr_images.");
+    CUTB_CUDA_OK(cudaSetDevice(0));
+    auto& b = image_buffers();
+    if (!b.ensure(0, ns * sizeof(float)) || !b.ensure(1, nc * sizeof(float)) || !b.ensure(2, nt * sizeof(float)))
+        return false;
+    CUTB_CUDA_OK(cudaMemcpy(b.ptr[2], template_image.data(), nt * sizeof(float), cudaMemcpyHostToDevice));
+    CUTB_CUDA_OK(cudaMemcpy(b.ptr[0], source_image.data(), ns * sizeof(float), cudaMemcpyHostToDevice));
+    if (!cutb_corr_images((const float*)b.ptr[2], (const float*)b.ptr[0], template_dims, source_dims,
+                          (float*)b.ptr[1], nullptr))
+        return false;
+    CUTB_CUDA_OK(cudaMemcpy(corr_map.data(), b.ptr[1], nc * sizeof(float), cudaMemcpyDeviceToHost));
+    return true;
 }
 
 // ---- C ABI ----------------------------------------------------------------------------------------
@@ -184,14 +254,30 @@ void beamform_f32_matlab(const float* data, CudaBeamformerParameters bp, float* 
         set_error(cutb_last_error(), "Error: Beamforming failed.");
 }
 
-void motion_detect_f32_matlab(const float*, NCCMotionParameters, float*)
+void motion_detect_f32_matlab(const float* images, NCCMotionParameters params, float* motion_maps)
 {
-    set_error(CUTB_ERR_UNSUPPORTED, "motion_detect_f32_matlab is not part of the RF -> volume library.");
+    // cuda_toolkit_matlab.cpp:39-52
+    const size_t in = sizeof(float) * (size_t)params.image_dims[0] * params.image_dims[1] * params.frame_count;
+    const size_t out =
+        4 * sizeof(float) * (size_t)params.motion_grid_dims[0] * params.motion_grid_dims[1] * params.frame_count;
+    if (!cuda_toolkit::motion_detection(std::span<const uint8_t>((const uint8_t*)images, in),
+                                        std::span<uint8_t>((uint8_t*)motion_maps, out), params))
+        set_error(cutb_last_error(), "Error: Motion detection failed.");
 }
 
-void corr_images_f32_matlab(const float*, const float*, CorrImagesParameters, float*)
+void corr_images_f32_matlab(const float* template_image, const float* source_image, CorrImagesParameters params,
+                            float* corr_map)
 {
-    set_error(CUTB_ERR_UNSUPPORTED, "corr_images_f32_matlab is not part of the RF -> volume library.");
+    // cuda_toolkit_matlab.cpp:54-76; sizes follow the dims (0 when the template is larger).
+    const size_t nt = (size_t)params.template_dims[0] * params.template_dims[1];
+    const size_t ns = (size_t)params.source_dims[0] * params.source_dims[1];
+    const bool fits = params.template_dims[0] <= params.source_dims[0] && params.template_dims[1] <= params.source_dims[1];
+    const size_t nc = fits ? (size_t)(params.source_dims[0] - params.template_dims[0] + 1) *
+                                 (params.source_dims[1] - params.template_dims[1] + 1)
+                           : 0;
+    if (!cuda_toolkit::corr_images(std::span<const float>(template_image, nt), std::span<const float>(source_image, ns),
+                                   std::span<float>(corr_map, nc), params.template_dims, params.source_dims))
+        set_error(cutb_last_error(), "Error: Correlation failed.");
 }
 
 bool init_cuda_configuration(const uint* input_dims, const uint* decoded_dims)

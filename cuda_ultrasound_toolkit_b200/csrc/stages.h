@@ -135,4 +135,16 @@ bool launch_das_direct(const DasArgs& a, const void* iq, bool iq_bf16, void* vol
 // Tile shape (x, y, z voxels) the delay-and-sum kernel uses for these arguments.
 void das_tile_shape(const DasArgs& a, int shape[3]);
 
+// ---- image correlation and block matching (motion.cu) --------------------------------------
+struct MotionArgs {
+    const float* frames;  // F images of W x H (x fastest)
+    float* maps;          // F x gy x gx float4
+    int W, H, F, patch, spacing, gx, gy, mx, my, ref, neighbour, subpixel;
+    float abs_thr, rel_thr, sharp_thr;
+    int tw_max, th_max, sw_max, sh_max, cw_max, ch_max;  // set by launch_block_match
+};
+bool launch_block_match(const MotionArgs& a, cudaStream_t st);
+bool launch_corr_images(const float* tpl, int tw, int th, const float* src, int sw, int sh, float* out,
+                        cudaStream_t st);
+
 }  // namespace cutb

@@ -123,3 +123,54 @@ class CudaBeamformerParameters(ctypes.Structure):
 
 
 assert ctypes.sizeof(CudaBeamformerParameters) == 8948
+
+
+class NccMotionParameters(ctypes.Structure):
+    """Block-matching parameters (cuda_beamformer_parameters.h:91-107 upstream). Index 0 of every
+    pair is the fastest image axis (x, the image width), index 1 the slow axis (y)."""
+
+    _fields_ = [
+        ("patch_size", _u),
+        ("motion_grid_spacing", _u),
+        ("motion_grid_dims", _u * 2),
+        ("scale_dims", _u * 2),
+        ("search_margins", _u * 2),
+        ("abs_cor_threshold", _f),
+        ("rel_cor_threshold", _f),
+        ("min_patch_variance", _f),
+        ("use_subpixel", ctypes.c_bool),
+        ("reference_frame", _u),
+        ("neighbour_compare", ctypes.c_bool),
+        ("frame_count", _u),
+        ("image_dims", _u * 2),
+        ("data_type", _i),
+    ]
+
+    FIELDS = ("patch_size", "motion_grid_spacing", "abs_cor_threshold", "rel_cor_threshold",
+              "min_patch_variance", "use_subpixel", "reference_frame", "neighbour_compare", "frame_count")
+    PAIRS = ("motion_grid_dims", "scale_dims", "search_margins", "image_dims")
+
+    @classmethod
+    def make(cls, **kw):
+        p = cls()
+        p.data_type = InputDataTypes.TYPE_F32
+        for k, v in kw.items():
+            if k in cls.PAIRS:
+                getattr(p, k)[0], getattr(p, k)[1] = int(v[0]), int(v[1])
+            else:
+                setattr(p, k, v)
+        return p
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k in self.FIELDS}
+        d.update({k: tuple(getattr(self, k)) for k in self.PAIRS})
+        return d
+
+
+class CorrImagesParameters(ctypes.Structure):
+    """Image sizes of corr_images_f32_matlab, index 0 = width (fastest axis)."""
+
+    _fields_ = [("template_dims", _u * 2), ("source_dims", _u * 2)]
+
+
+assert ctypes.sizeof(NccMotionParameters) == 72

@@ -205,3 +205,23 @@ def phantom(rng, n_points, n_speckle=0, speckle_sigma=0.05, box_xy=9e-3, z_range
     out[:n_points, 3] = rng.uniform(0.5, 1.0, n_points)
     out[n_points:, 3] = rng.normal(0.0, speckle_sigma, n_speckle)
     return out
+
+
+def speckle_frames(seed, width, height, shifts, noise=2.0, sigma=1.4, pad=24):
+    """8-bit B-mode-like frames [F][height][width] (uint8): the envelope of one band-limited complex
+    speckle field, frame k translated by shifts[k] = (dx, dy) pixels (Fourier shift, so sub-pixel
+    shifts are exact band-limited translations), plus Gaussian noise. Inputs of the image
+    correlation and motion-detection entry points."""
+    rng = np.random.default_rng(seed)
+    H, W = height + 2 * pad, width + 2 * pad
+    field = rng.standard_normal((H, W)) + 1j * rng.standard_normal((H, W))
+    ky = np.fft.fftfreq(H)[:, None]
+    kx = np.fft.fftfreq(W)[None, :]
+    spec = np.fft.fft2(field) * np.exp(-2 * (np.pi * sigma) ** 2 * (kx ** 2 + ky ** 2))
+    frames = []
+    for dx, dy in shifts:
+        env = np.abs(np.fft.ifft2(spec * np.exp(-2j * np.pi * (kx * dx + ky * dy))))[pad:pad + height, pad:pad + width]
+        frames.append(env)
+    frames = np.stack(frames)
+    frames = frames / np.percentile(frames, 99.5) * 230.0 + rng.normal(0.0, noise, frames.shape)
+    return np.clip(np.rint(frames), 0, 255).astype(np.uint8)

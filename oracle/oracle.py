@@ -27,8 +27,10 @@ def lib():
         L.orc_convert_decode_f64.argtypes = [vp, i, u, u, u, u, u, vp, i, vp, i]
         L.orc_hilbert.argtypes = [vp, ctypes.c_size_t, u, vp, u, vp, i]
         L.orc_das.argtypes = [vp, vp, vp, ctypes.c_size_t, vp, i]
+        L.orc_corr_images.argtypes = [vp, u, u, vp, u, u, vp]
+        L.orc_motion_detection.argtypes = [vp, vp, vp, i]
         for f in (L.orc_encoding_matrix, L.orc_convert_decode_i16, L.orc_convert_decode_f64, L.orc_hilbert,
-                  L.orc_das):
+                  L.orc_das, L.orc_corr_images, L.orc_motion_detection):
             f.restype = i
         _lib = L
     return _lib
@@ -141,3 +143,23 @@ def convert_demod(raw, bp, taps=None):
         acc[..., lo:hi] += z[..., lo + i - half:hi + i - half] * h[L - 1 - i]
         cnt[lo:hi] += 1
     return acc / cnt
+
+
+def corr_images(template, source):
+    """Zero-mean normalised cross-correlation, valid positions: (hs - ht + 1, ws - wt + 1)."""
+    t = np.ascontiguousarray(template, dtype=np.float32)
+    s = np.ascontiguousarray(source, dtype=np.float32)
+    (th, tw), (sh, sw) = t.shape, s.shape
+    out = np.empty((sh - th + 1, sw - tw + 1), dtype=np.float32)
+    _ok(lib().orc_corr_images(t.ctypes.data, tw, th, s.ctypes.data, sw, sh, out.ctypes.data), "image sizes")
+    return out
+
+
+def motion_detection(frames, params, threads=0):
+    """Block-matching motion maps [frame][grid y][grid x][dx, dy, peak, no-shift peak]."""
+    f = np.ascontiguousarray(frames, dtype=np.float32)
+    gx, gy = int(params.motion_grid_dims[0]), int(params.motion_grid_dims[1])
+    out = np.empty((int(params.frame_count), gy, gx, 4), dtype=np.float32)
+    _ok(lib().orc_motion_detection(f.ctypes.data, ctypes.addressof(params), out.ctypes.data, threads),
+        "motion parameters")
+    return out

@@ -48,6 +48,23 @@ def test_header_layout_compiles(tmp_path, lang):
     assert subprocess.run([str(exe)]).returncode == 0
 
 
+def test_motion_parameter_layout(tmp_path):
+    """NccMotionParameters / CorrImagesParameters: the ctypes mirrors match the C header."""
+    from cuda_ultrasound_toolkit_b200.params import CorrImagesParameters, NccMotionParameters
+    fields = [f[0] for f in NccMotionParameters._fields_]
+    src = tmp_path / "m.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "cuda_beamformer_parameters.h"\n'
+                   "int main(void) {\n"
+                   + "".join(f'printf("%zu\\n", offsetof(NCCMotionParameters, {f}));\n' for f in fields)
+                   + 'printf("%zu\\n%zu\\n", sizeof(NCCMotionParameters), sizeof(CorrImagesParameters));\n'
+                   "return 0; }\n")
+    exe = tmp_path / "m"
+    subprocess.run(["gcc", "-std=c11", "-I", INCLUDE, str(src), "-o", str(exe)], check=True)
+    vals = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
+    assert vals[:-2] == [getattr(NccMotionParameters, f).offset for f in fields]
+    assert vals[-2:] == [ctypes.sizeof(NccMotionParameters), ctypes.sizeof(CorrImagesParameters)]
+
+
 def _declared_functions():
     names = set()
     for fn in os.listdir(INCLUDE):

@@ -100,3 +100,47 @@ def test_bandpass_front_end_matches_upstream(orc):
         got = orc.convert_demod(g[n + ".raw"], bp, taps if len(taps) else None)
         want = g[n + ".iq"]
         assert np.linalg.norm(got - want) / np.linalg.norm(want) < 1e-4, n
+
+
+# ---- image correlation and NCC motion detection (tests/golden/make_ncc_golden.py, on a GPU) -------
+# Upstream's correlation is NPP's FP32 nppiCrossCorrValid_NormLevel_32f_C1R; the oracle forms it in
+# FP64. Measured oracle-vs-upstream: correlation values <= 3.6e-6, motion vectors <= 7e-6.
+TOL_CORR_UPSTREAM = 2e-5
+TOL_MOTION_UPSTREAM = 1e-4
+
+
+def test_corr_images_oracle_matches_upstream(orc):
+    from tests import ncc_golden as N
+    g = N.load()
+    names = N.cases(g, "corr")
+    assert len(names) == 7
+    for name in names:
+        t, s, ref = N.corr_case(g, name)
+        out = orc.corr_images(t, s)
+        assert out.shape == ref.shape, name
+        flat = ref >= N.FLT_MAX  # zero-variance positions: NPP returns FLT_MAX
+        assert ((out >= N.FLT_MAX) == flat).all(), name
+        assert np.abs(out[~flat] - ref[~flat]).max(initial=0) < TOL_CORR_UPSTREAM, name
+    # the flat cases exercise both zero-variance forms
+    assert (N.corr_case(g, "flat_template")[2] >= N.FLT_MAX).all()
+    ref = N.corr_case(g, "flat_block")[2]
+    assert 0 < (ref >= N.FLT_MAX).sum() < ref.size
+
+
+def test_motion_oracle_matches_upstream(orc):
+    from tests import ncc_golden as N
+    g = N.load()
+    names = N.cases(g, "motion")
+    assert len(names) == 5
+    for name in names:
+        frames, p, ref = N.motion_case(g, name)
+        out = orc.motion_detection(frames, p)
+        assert out.shape == ref.shape, name
+        assert np.abs(out - ref).max() < TOL_MOTION_UPSTREAM, name
+        # the reference frame keeps its cleared map
+        assert (out[p.reference_frame] == 0).all()
+    # the cases cover accepted vectors, rejected peaks (-1) and sub-pixel offsets
+    _, _, m = N.motion_case(g, "tiny_search_strict")
+    assert (m[..., 2] == -1).any() and (m[..., 2] > 0).any()
+    _, _, m = N.motion_case(g, "subpixel_ref0")
+    assert (np.abs(m[..., 0] - np.rint(m[..., 0])) > 0.05).any()
