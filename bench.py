@@ -495,17 +495,11 @@ def motion_section(reps=10, warmup=3):
     import torch
     from cuda_ultrasound_toolkit_b200 import api
     from cuda_ultrasound_toolkit_b200.params import NccMotionParameters
-    from cuda_ultrasound_toolkit_b200.synth import speckle_frames
     from oracle import oracle as O
+    from cuda_ultrasound_toolkit_b200.synth import motion_workload
     W = H = 512
     F, P, sp, G, M = 16, 32, 16, 32, 16
-    rng = np.random.default_rng(77)
-    shifts = [(0.0, 0.0)] + [tuple(rng.uniform(-10, 10, 2)) for _ in range(F - 1)]
-    frames = speckle_frames(2024, W, H, shifts).astype(np.float32)
-    p = NccMotionParameters.make(frame_count=F, image_dims=(W, H), patch_size=P, motion_grid_spacing=sp,
-                                 motion_grid_dims=(G, G), search_margins=(M, M), abs_cor_threshold=0.3,
-                                 rel_cor_threshold=0.0, min_patch_variance=0.0, use_subpixel=True,
-                                 reference_frame=0, neighbour_compare=False)
+    frames, p = motion_workload(F, W, P, sp, G, M)
     vectors = (F - 1) * G * G
     # algorithmic FLOPs of the correlation numerators (2 per template pixel per map position),
     # window by window with the border clipping

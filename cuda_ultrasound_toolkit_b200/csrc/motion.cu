@@ -35,7 +35,6 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kCandidates = 32;     // find_peaks_kernel keeps the first 32 ranks
 constexpr int kPerThread = 8;       // ... of 256 threads x 8 loaded map values
-constexpr int kStrip = 4;           // correlation outputs per thread along x
 constexpr double kFlatTol = 1e-11;  // relative size of n*var below which a window counts as flat
 constexpr size_t kMaxSmem = 200 * 1024;
 
@@ -110,59 +109,138 @@ __device__ __forceinline__ Window cell_window(const MotionArgs& a, int col, int 
     return w;
 }
 
-// Correlation map of the staged template (centred, tsm) over the staged window (ssm, row stride
-// sws, shifted by c), FP64 row sums in h1/h2. Leaves cmap complete (after a barrier).
-__device__ void corr_map_smem(const float* ssm, int sws, const float* tsm, int tw, int th, int cw, int ch,
-                              double tvar, double* h1, double* h2, float* cmap)
+// Correlation map of the staged template (centred, tsm, row stride tws, zero beyond tw) over the
+// staged window (ssm, row stride sws, shifted by c, zero beyond sw). Leaves cmap complete (after
+// a barrier); h1/h2 (sh x cw doubles each) are scratch.
+//
+// Warps 0-1 form the window moments while warps 2-7 accumulate the numerators into cmap; then
+// every thread turns numerator and moments into the coefficient.
+//
+// Window moments: FP64 running sums along each row, then down each column in place, so that
+// h1/h2[oy][ox] end as sum S_c and sum S_c^2 over the window at (ox, oy). Exact for
+// integer-valued images; otherwise ~1e-15 relative.
+//
+// Numerator: each thread accumulates a strip of 8 consecutive map positions of one row; per 4
+// template columns it loads 4 new window values and 4 template values as float4 and issues 32
+// FMAs (the template-column loop is unrolled completely for 16- and 32-wide templates).
+// Consecutive lanes take consecutive rows; the row stride is 4 (mod 8) words, so the 8 lanes of
+// a 16-byte load phase hit 8 different bank quads.
+constexpr int kStrip = 8;
+constexpr int kMomentWarps = 2;
+constexpr int kMomentThreads = 32 * kMomentWarps;
+
+__device__ __forceinline__ void strip_fma(float (&acc)[kStrip], const float4& a, const float4& b, const float4& c,
+                                          const float4& t)
+{
+    const float w[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
+    const float tv[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+    for (int qq = 0; qq < 4; ++qq)
+#pragma unroll
+        for (int k = 0; k < kStrip; ++k) acc[k] = fmaf(w[k + qq], tv[qq], acc[k]);
+}
+
+// QB = template float4 columns when known at compile time, 0 for any width.
+template <int QB>
+__device__ __forceinline__ void numerator_strips(const float* ssm, int sws, const float* tsm, int tws, int th, int cw,
+                                                 int ch, int qblocks, float* cmap, int tid, int nthreads)
+{
+    const int nsx = (cw + kStrip - 1) / kStrip;
+    for (int j = tid; j < nsx * ch; j += nthreads) {
+        const int oy = j % ch, ox0 = (j / ch) * kStrip;
+        float acc[kStrip];
+#pragma unroll
+        for (int k = 0; k < kStrip; ++k) acc[k] = 0.f;
+        for (int r = 0; r < th; ++r) {
+            const float4* srow = reinterpret_cast<const float4*>(ssm + (oy + r) * sws + ox0);
+            const float4* trow = reinterpret_cast<const float4*>(tsm + r * tws);
+            float4 a = srow[0], b = srow[1];
+            if constexpr (QB > 0) {
+#pragma unroll
+                for (int qb = 0; qb < QB; ++qb) {
+                    const float4 c = srow[qb + 2];
+                    strip_fma(acc, a, b, c, trow[qb]);
+                    a = b;
+                    b = c;
+                }
+            } else {
+                for (int qb = 0; qb < qblocks; ++qb) {
+                    const float4 c = srow[qb + 2];
+                    strip_fma(acc, a, b, c, trow[qb]);
+                    a = b;
+                    b = c;
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kStrip; ++k)
+            if (ox0 + k < cw) cmap[oy * cw + ox0 + k] = acc[k];
+    }
+}
+
+__device__ void window_moments(const float* ssm, int sws, int tw, int th, int cw, int ch, double* h1, double* h2,
+                               int tid)
 {
     const int sh = ch + th - 1;
-    // row moments of every tw-wide run: h[y][ox] = sum_q S_c[y][ox + q] (and squares)
-    for (int i = threadIdx.x; i < sh * cw; i += kThreads) {
-        const int y = i / cw, ox = i - y * cw;
-        const float* r = ssm + y * sws + ox;
+    for (int y = tid; y < sh; y += kMomentThreads) {
+        const float* r = ssm + y * sws;
         double a = 0, b = 0;
         for (int q = 0; q < tw; ++q) {
             const double v = r[q];
             a += v;
             b = fma(v, v, b);
         }
-        h1[i] = a;
-        h2[i] = b;
+        h1[y * cw] = a;
+        h2[y * cw] = b;
+        for (int ox = 1; ox < cw; ++ox) {
+            const double vin = r[ox + tw - 1], vout = r[ox - 1];
+            a += vin - vout;
+            b += fma(vin, vin, -vout * vout);
+            h1[y * cw + ox] = a;
+            h2[y * cw + ox] = b;
+        }
+    }
+    asm volatile("bar.sync 1, %0;" ::"n"(kMomentThreads) : "memory");
+    for (int ox = tid; ox < cw; ox += kMomentThreads) {
+        double a = 0, b = 0;
+        for (int r = 0; r < th; ++r) {
+            a += h1[r * cw + ox];
+            b += h2[r * cw + ox];
+        }
+        for (int oy = 0; oy < ch; ++oy) {
+            const int i = oy * cw + ox;
+            double na = a, nb = b;
+            if (oy + 1 < ch) {
+                na += h1[i + th * cw] - h1[i];
+                nb += h2[i + th * cw] - h2[i];
+            }
+            h1[i] = a;  // row oy is not read again by this column
+            h2[i] = b;
+            a = na;
+            b = nb;
+        }
+    }
+}
+
+__device__ void corr_map_smem(const float* ssm, int sws, const float* tsm, int tws, int tw, int th, int cw, int ch,
+                              double tvar, double* h1, double* h2, float* cmap)
+{
+    const int warp = threadIdx.x >> 5;
+    if (warp < kMomentWarps) {
+        window_moments(ssm, sws, tw, th, cw, ch, h1, h2, threadIdx.x);
+    } else {
+        const int tid = threadIdx.x - kMomentThreads, nt = kThreads - kMomentThreads;
+        const int qblocks = tws / 4;
+        if (qblocks == 8)
+            numerator_strips<8>(ssm, sws, tsm, tws, th, cw, ch, qblocks, cmap, tid, nt);
+        else if (qblocks == 4)
+            numerator_strips<4>(ssm, sws, tsm, tws, th, cw, ch, qblocks, cmap, tid, nt);
+        else
+            numerator_strips<0>(ssm, sws, tsm, tws, th, cw, ch, qblocks, cmap, tid, nt);
     }
     __syncthreads();
     const double n = (double)tw * th;
-    const int nsx = (cw + kStrip - 1) / kStrip;
-    for (int j = threadIdx.x; j < nsx * ch; j += kThreads) {
-        const int oy = j / nsx, ox0 = (j - oy * nsx) * kStrip;
-        float acc[kStrip] = {0.f, 0.f, 0.f, 0.f};
-        for (int r = 0; r < th; ++r) {
-            const float* srow = ssm + (oy + r) * sws + ox0;
-            const float* trow = tsm + r * tw;
-            float s0 = srow[0], s1 = srow[1], s2 = srow[2];
-            for (int q = 0; q < tw; ++q) {
-                const float s3 = srow[q + 3];
-                const float t = trow[q];
-                acc[0] = fmaf(s0, t, acc[0]);
-                acc[1] = fmaf(s1, t, acc[1]);
-                acc[2] = fmaf(s2, t, acc[2]);
-                acc[3] = fmaf(s3, t, acc[3]);
-                s0 = s1;
-                s1 = s2;
-                s2 = s3;
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < kStrip; ++k) {
-            const int ox = ox0 + k;
-            if (ox >= cw) break;
-            double m1 = 0, m2 = 0;
-            for (int r = 0; r < th; ++r) {
-                m1 += h1[(oy + r) * cw + ox];
-                m2 += h2[(oy + r) * cw + ox];
-            }
-            cmap[oy * cw + ox] = ncc_value(acc[k], m1, m2, n, tvar);
-        }
-    }
+    for (int i = threadIdx.x; i < cw * ch; i += kThreads) cmap[i] = ncc_value(cmap[i], h1[i], h2[i], n, tvar);
     __syncthreads();
 }
 
@@ -189,18 +267,19 @@ __device__ void select_candidates(const float* cmap, int n, int* cand, unsigned 
                 key[j - 1] = t;
             }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // 64-bit maximum from two 32-bit warp reductions: high words, then low words among the
+    // lanes holding the highest high word.
+    auto warp_max = [](unsigned long long v) {
+        const uint32_t hi = (uint32_t)(v >> 32), lo = (uint32_t)v;
+        const uint32_t mh = __reduce_max_sync(0xffffffffu, hi);
+        const uint32_t ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
+        return ((unsigned long long)mh << 32) | ml;
+    };
     for (int round = 0; round < kCandidates; ++round) {
-        unsigned long long m = key[0];
-#pragma unroll
-        for (int o = 16; o; o >>= 1) {
-            const unsigned long long x = __shfl_xor_sync(0xffffffffu, m, o);
-            m = x > m ? x : m;
-        }
+        const unsigned long long m = warp_max(key[0]);
         if (lane == 0) wbuf[round & 1][warp] = m;
         __syncthreads();
-        unsigned long long best = wbuf[round & 1][0];
-#pragma unroll
-        for (int w = 1; w < kWarps; ++w) best = wbuf[round & 1][w] > best ? wbuf[round & 1][w] : best;
+        const unsigned long long best = warp_max(wbuf[round & 1][lane & (kWarps - 1)]);
         if (key[0] == best) {  // keys are unique (index part)
 #pragma unroll
             for (int i = 0; i + 1 < kPerThread; ++i) key[i] = key[i + 1];
@@ -278,23 +357,27 @@ __device__ void test_candidates(const float* cmap, int cw, int ch, const int* ca
 
 struct MotionSmem {
     size_t h_off, s_off, t_off, c_off, bytes;
-    int sws;
+    int sws, tws;
 };
 
+// Window rows hold the strips' overrun (up to index sw + 10) at a stride of 4 (mod 8) words; template
+// rows are padded to whole float4s.
 __host__ __device__ inline MotionSmem motion_smem(const MotionArgs& a)
 {
     MotionSmem m;
     const int sw = a.sw_max, sh = a.sh_max, cw = a.cw_max, ch = a.ch_max;
-    m.sws = sw + kStrip - 1;
+    const int base = sw + 11;  // strips read up to index sw + 10
+    m.sws = base + (12 - base % 8) % 8;  // smallest stride >= base that is 4 (mod 8)
+    m.tws = (a.tw_max + 3) / 4 * 4;
     m.h_off = 0;
     m.s_off = m.h_off + 2 * sizeof(double) * (size_t)sh * cw;
     m.t_off = m.s_off + sizeof(float) * (size_t)sh * m.sws;
-    m.c_off = m.t_off + sizeof(float) * (size_t)a.tw_max * a.th_max;
+    m.c_off = m.t_off + sizeof(float) * (size_t)m.tws * a.th_max;
     m.bytes = m.c_off + sizeof(float) * (size_t)cw * ch;
     return m;
 }
 
-__global__ void __launch_bounds__(kThreads) block_match_kernel(MotionArgs a)
+__global__ void __launch_bounds__(kThreads, 3) block_match_kernel(MotionArgs a)
 {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ double red[kWarps];
@@ -323,19 +406,20 @@ __global__ void __launch_bounds__(kThreads) block_match_kernel(MotionArgs a)
     const size_t frame_px = (size_t)a.W * a.H;
     const float* T = a.frames + (size_t)tf * frame_px + (size_t)w.tt * a.W + w.tl;
     const float* S = a.frames + (size_t)f * frame_px + (size_t)w.st * a.W + w.sl;
-    const int nt = w.tw * w.th;
+    const int nt = w.tw * w.th, tws = (w.tw + 3) / 4 * 4;
     double part = 0;
-    for (int i = threadIdx.x; i < nt; i += kThreads) {
-        const int y = i / w.tw, x = i - y * w.tw;
-        const float v = __ldg(T + (size_t)y * a.W + x);
+    for (int i = threadIdx.x; i < w.th * tws; i += kThreads) {
+        const int y = i / tws, x = i - y * tws;
+        const float v = x < w.tw ? __ldg(T + (size_t)y * a.W + x) : 0.f;
         tsm[i] = v;
         part += v;
     }
     const double mean = block_sum(part, red) / (double)nt;
     const float shift = rintf((float)mean);
     part = 0;
-    for (int i = threadIdx.x; i < nt; i += kThreads) {
-        const float d = (float)((double)tsm[i] - mean);
+    for (int i = threadIdx.x; i < w.th * tws; i += kThreads) {
+        const int x = i % tws;
+        const float d = x < w.tw ? (float)((double)tsm[i] - mean) : 0.f;
         tsm[i] = d;
         part = fma((double)d, (double)d, part);
     }
@@ -345,7 +429,7 @@ __global__ void __launch_bounds__(kThreads) block_match_kernel(MotionArgs a)
         ssm[i] = x < w.sw ? __ldg(S + (size_t)y * a.W + x) - shift : 0.f;
     }
     __syncthreads();
-    corr_map_smem(ssm, L.sws, tsm, w.tw, w.th, cw, ch, tvar, h1, h2, cmap);
+    corr_map_smem(ssm, L.sws, tsm, tws, w.tw, w.th, cw, ch, tvar, h1, h2, cmap);
     select_candidates(cmap, cw * ch, cand, wbuf);
     if (threadIdx.x < 32)
         test_candidates(cmap, cw, ch, cand, w.tl - w.sl, w.tt - w.st, a,
@@ -355,6 +439,7 @@ __global__ void __launch_bounds__(kThreads) block_match_kernel(MotionArgs a)
 // ---- corr_images: template statistics, window row moments, tiled correlation ------------------
 
 constexpr int kTileX = 64, kTileY = 16;   // outputs per CTA (256 threads x 4 along x)
+constexpr int kTileStrip = 4;
 constexpr int kChunkX = 32, kChunkY = 16; // template block staged per step
 
 struct TplStats {
@@ -411,15 +496,15 @@ __global__ void __launch_bounds__(kThreads) corr_tile_kernel(const float* __rest
                                                              const TplStats* st, const double2* __restrict__ h,
                                                              float* __restrict__ out)
 {
-    constexpr int kSW = kTileX + kChunkX - 1 + kStrip - 1;  // staged window width (with strip overrun)
+    constexpr int kSW = kTileX + kChunkX - 1 + kTileStrip - 1;  // staged window width (with strip overrun)
     constexpr int kSH = kTileY + kChunkY - 1;
     __shared__ float ssm[kSH][kSW];
     __shared__ float tsm[kChunkY][kChunkX];
     const int cw = sw - tw + 1, ch = sh - th + 1;
     const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY;
-    const int tx = threadIdx.x % (kTileX / kStrip), ty = threadIdx.x / (kTileX / kStrip);
+    const int tx = threadIdx.x % (kTileX / kTileStrip), ty = threadIdx.x / (kTileX / kTileStrip);
     const float c = st->shift;
-    float acc[kStrip] = {0.f, 0.f, 0.f, 0.f};
+    float acc[kTileStrip] = {0.f, 0.f, 0.f, 0.f};
     for (int r0 = 0; r0 < th; r0 += kChunkY)
         for (int q0 = 0; q0 < tw; q0 += kChunkX) {
             const int rn = min(kChunkY, th - r0), qn = min(kChunkX, tw - q0);
@@ -435,7 +520,7 @@ __global__ void __launch_bounds__(kThreads) corr_tile_kernel(const float* __rest
             }
             __syncthreads();
             for (int r = 0; r < rn; ++r) {
-                const float* srow = &ssm[ty + r][tx * kStrip];
+                const float* srow = &ssm[ty + r][tx * kTileStrip];
                 float s0 = srow[0], s1 = srow[1], s2 = srow[2];
                 for (int q = 0; q < qn; ++q) {
                     const float s3 = srow[q + 3];
@@ -454,8 +539,8 @@ __global__ void __launch_bounds__(kThreads) corr_tile_kernel(const float* __rest
     if (oy >= ch) return;
     const double n = (double)tw * th, tvar = st->tvar;
 #pragma unroll
-    for (int k = 0; k < kStrip; ++k) {
-        const int ox = x0 + tx * kStrip + k;
+    for (int k = 0; k < kTileStrip; ++k) {
+        const int ox = x0 + tx * kTileStrip + k;
         if (ox >= cw) break;
         double m1 = 0, m2 = 0;
         for (int r = 0; r < th; ++r) {

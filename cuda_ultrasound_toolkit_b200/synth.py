@@ -225,3 +225,19 @@ def speckle_frames(seed, width, height, shifts, noise=2.0, sigma=1.4, pad=24):
     frames = np.stack(frames)
     frames = frames / np.percentile(frames, 99.5) * 230.0 + rng.normal(0.0, noise, frames.shape)
     return np.clip(np.rint(frames), 0, 255).astype(np.uint8)
+
+
+def motion_workload(frames=16, size=512, patch=32, spacing=16, grid=32, margin=16, seed=2024):
+    """The motion-detection benchmark case: `frames` speckle frames of size x size, frame k > 0
+    translated by a seeded shift of up to 10 px from frame 0; patch / grid / search as given, every
+    frame against frame 0. Returns (frames float32 [F][H][W], NccMotionParameters)."""
+    from .params import NccMotionParameters
+    rng = np.random.default_rng(77)
+    shifts = [(0.0, 0.0)] + [tuple(rng.uniform(-10, 10, 2)) for _ in range(frames - 1)]
+    f = speckle_frames(seed, size, size, shifts).astype(np.float32)
+    p = NccMotionParameters.make(frame_count=frames, image_dims=(size, size), patch_size=patch,
+                                 motion_grid_spacing=spacing, motion_grid_dims=(grid, grid),
+                                 search_margins=(margin, margin), abs_cor_threshold=0.3, rel_cor_threshold=0.0,
+                                 min_patch_variance=0.0, use_subpixel=True, reference_frame=0,
+                                 neighbour_compare=False)
+    return f, p
