@@ -59,11 +59,15 @@ __device__ double block_sum(double v, double* red)
     return s;
 }
 
-__device__ __forceinline__ float ncc_value(float num, double s1, double s2, double n, double tvar)
+// num / sqrt(var_S * var_T) with d = n * sum (S - mean S)^2 and tvn = sum T'^2 / n; the flat test
+// in FP64, the final scale in FP32 (~3e-7 relative) unless the product leaves the FP32 range.
+__device__ __forceinline__ float ncc_value(float num, double s1, double s2, double n, double tvn)
 {
-    const double d = n * s2 - s1 * s1;  // n * sum (S - mean S)^2
-    if (tvar <= 0.0 || d <= kFlatTol * n * s2) return FLT_MAX;
-    return (float)((double)num / sqrt(d / n * tvar));
+    const double d = n * s2 - s1 * s1;
+    if (tvn <= 0.0 || d <= kFlatTol * n * s2) return FLT_MAX;
+    const double x = d * tvn;
+    if (x > 1e-30 && x < 1e30) return num * rsqrtf((float)x);
+    return (float)((double)num / sqrt(x));
 }
 
 // Quadratic-surface weights on the 3 x 3 grid (x, y in {-1, 0, 1}) for the coefficients of
@@ -239,8 +243,8 @@ __device__ void corr_map_smem(const float* ssm, int sws, const float* tsm, int t
             numerator_strips<0>(ssm, sws, tsm, tws, th, cw, ch, qblocks, cmap, tid, nt);
     }
     __syncthreads();
-    const double n = (double)tw * th;
-    for (int i = threadIdx.x; i < cw * ch; i += kThreads) cmap[i] = ncc_value(cmap[i], h1[i], h2[i], n, tvar);
+    const double n = (double)tw * th, tvn = tvar / n;
+    for (int i = threadIdx.x; i < cw * ch; i += kThreads) cmap[i] = ncc_value(cmap[i], h1[i], h2[i], n, tvn);
     __syncthreads();
 }
 
@@ -407,27 +411,27 @@ __global__ void __launch_bounds__(kThreads, 3) block_match_kernel(MotionArgs a)
     const float* T = a.frames + (size_t)tf * frame_px + (size_t)w.tt * a.W + w.tl;
     const float* S = a.frames + (size_t)f * frame_px + (size_t)w.st * a.W + w.sl;
     const int nt = w.tw * w.th, tws = (w.tw + 3) / 4 * 4;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double part = 0;
-    for (int i = threadIdx.x; i < w.th * tws; i += kThreads) {
-        const int y = i / tws, x = i - y * tws;
-        const float v = x < w.tw ? __ldg(T + (size_t)y * a.W + x) : 0.f;
-        tsm[i] = v;
-        part += v;
-    }
+    for (int y = warp; y < w.th; y += kWarps)
+        for (int x = lane; x < tws; x += 32) {
+            const float v = x < w.tw ? __ldg(T + (size_t)y * a.W + x) : 0.f;
+            tsm[y * tws + x] = v;
+            part += v;
+        }
     const double mean = block_sum(part, red) / (double)nt;
     const float shift = rintf((float)mean);
     part = 0;
-    for (int i = threadIdx.x; i < w.th * tws; i += kThreads) {
-        const int x = i % tws;
-        const float d = x < w.tw ? (float)((double)tsm[i] - mean) : 0.f;
-        tsm[i] = d;
-        part = fma((double)d, (double)d, part);
-    }
+    for (int y = warp; y < w.th; y += kWarps)
+        for (int x = lane; x < w.tw; x += 32) {
+            const float d = (float)((double)tsm[y * tws + x] - mean);
+            tsm[y * tws + x] = d;
+            part = fma((double)d, (double)d, part);
+        }
     const double tvar = block_sum(part, red);
-    for (int i = threadIdx.x; i < w.sh * L.sws; i += kThreads) {
-        const int y = i / L.sws, x = i - y * L.sws;
-        ssm[i] = x < w.sw ? __ldg(S + (size_t)y * a.W + x) - shift : 0.f;
-    }
+    for (int y = warp; y < w.sh; y += kWarps)
+        for (int x = lane; x < L.sws; x += 32)
+            ssm[y * L.sws + x] = x < w.sw ? __ldg(S + (size_t)y * a.W + x) - shift : 0.f;
     __syncthreads();
     corr_map_smem(ssm, L.sws, tsm, tws, w.tw, w.th, cw, ch, tvar, h1, h2, cmap);
     select_candidates(cmap, cw * ch, cand, wbuf);
@@ -537,7 +541,7 @@ __global__ void __launch_bounds__(kThreads) corr_tile_kernel(const float* __rest
         }
     const int oy = y0 + ty;
     if (oy >= ch) return;
-    const double n = (double)tw * th, tvar = st->tvar;
+    const double n = (double)tw * th, tvn = st->tvar / n;
 #pragma unroll
     for (int k = 0; k < kTileStrip; ++k) {
         const int ox = x0 + tx * kTileStrip + k;
@@ -548,7 +552,7 @@ __global__ void __launch_bounds__(kThreads) corr_tile_kernel(const float* __rest
             m1 += v.x;
             m2 += v.y;
         }
-        out[(size_t)oy * cw + ox] = ncc_value(acc[k], m1, m2, n, tvar);
+        out[(size_t)oy * cw + ox] = ncc_value(acc[k], m1, m2, n, tvn);
     }
 }
 
