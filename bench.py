@@ -327,6 +327,11 @@ def run_ours(args, rank, world, local_rank):
             line["motion"] = motion_section()
         except Exception as exc:  # must not hide the plain pipeline's number
             line["motion"] = {"failed": str(exc)}
+    if args.transfer and world == 1:
+        try:
+            line["transfer"] = transfer_section()
+        except Exception as exc:  # must not hide the plain pipeline's number
+            line["transfer"] = {"failed": str(exc)}
     try:
         per_vol, sample = cpu_sample(frames[0][0], bp, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": 1.0 / per_vol, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
@@ -578,6 +583,42 @@ def motion_section(reps=10, warmup=3):
     return out
 
 
+def transfer_section(reps=5):
+    """The out-of-process path on the full workload: beamform_i16 from libcuda_transfer.so to a
+    cutb_transfer_server process (shared-memory input and output, command socket), against the
+    same request through cuda_toolkit::beamform in this process. Wall-clock per volume, both
+    with host buffers."""
+    import time
+    import uuid
+    from cuda_ultrasound_toolkit_b200 import api, synth, transfer
+    raw, bp = synth.frame("full")
+    name = "cutbb" + uuid.uuid4().hex[:8]
+    os.environ["CUDA_TRANSFER_NAME"] = name
+    transfer.set_timeout_ms(600000)
+    proc = transfer.spawn_server(name, data_bytes=256 << 20, timeout_ms=600000)
+    try:
+        out = np.empty(bp.volume_shape, np.complex64)
+        transfer.beamform_i16(raw, bp, out=out)
+        t = time.perf_counter()
+        for _ in range(reps):
+            transfer.beamform_i16(raw, bp, out=out)
+        ipc_ms = (time.perf_counter() - t) / reps * 1e3
+    finally:
+        transfer.deinit()
+        proc.terminate()
+        proc.wait(30)
+        os.environ.pop("CUDA_TRANSFER_NAME", None)
+    ref = api.beamform(raw, bp)
+    t = time.perf_counter()
+    for _ in range(reps):
+        api.beamform(raw, bp, out=ref)
+    direct_ms = (time.perf_counter() - t) / reps * 1e3
+    return {"workload": "full frame via the command socket + shared memory to a server process",
+            "ipc_ms": ipc_ms, "ipc_volumes_per_s": 1e3 / ipc_ms, "direct_ms": direct_ms,
+            "direct_volumes_per_s": 1e3 / direct_ms, "identical": bool(np.array_equal(out, ref)),
+            "bytes_in": int(raw.nbytes), "bytes_out": int(out.nbytes)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -589,6 +630,7 @@ def main():
     ap.add_argument("--batched", type=int, default=64, help="frames of the batched mixed-size stream (0: skip)")
     ap.add_argument("--precision", type=int, default=1, help="run the 256 x 256 x 8192 precision form (0: skip)")
     ap.add_argument("--motion", type=int, default=1, help="run the NCC motion-detection section (0: skip)")
+    ap.add_argument("--transfer", type=int, default=1, help="run the out-of-process transfer section (0: skip)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -65,10 +65,10 @@ def test_motion_parameter_layout(tmp_path):
     assert vals[-2:] == [ctypes.sizeof(NccMotionParameters), ctypes.sizeof(CorrImagesParameters)]
 
 
-def _declared_functions():
+def _declared_functions(only=None, skip=("cuda_transfer.h",)):
     names = set()
     for fn in os.listdir(INCLUDE):
-        if not fn.endswith(".h"):
+        if not fn.endswith(".h") or (only and fn != only) or (not only and fn in skip):
             continue
         text = open(os.path.join(INCLUDE, fn)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
@@ -87,6 +87,19 @@ def test_library_exports_every_declared_symbol(native):
     out = subprocess.run(["nm", "-DC", "--defined-only", native._name], capture_output=True, text=True).stdout
     for sym in ("cuda_toolkit::beamform(", "cuda_toolkit::motion_detection(", "cuda_toolkit::corr_images("):
         assert sym in out, sym
+
+
+def test_transfer_client_exports_every_declared_symbol(native):
+    """cuda_transfer.h (the drop-in of upstream's client library) is implemented by
+    libcuda_transfer.so, a plain C library with no CUDA dependency."""
+    from cuda_ultrasound_toolkit_b200 import transfer
+    declared = _declared_functions(only="cuda_transfer.h")
+    assert {"beamform_i16", "beamform_f32", "motion_detect_f32", "corr_images_f32", "deinit"} <= declared
+    client = transfer.client()
+    for name in declared:
+        assert hasattr(client, name), name
+    out = subprocess.run(["ldd", transfer.CLIENT_PATH], capture_output=True, text=True).stdout
+    assert "cuda" not in out.replace("libcuda_transfer", "")
 
 
 def test_library_links_no_fft_or_blas(native):
