@@ -291,7 +291,8 @@ class Plan:
         import torch  # noqa: F401  (device memory comes from torch)
         self.bp = bp.copy()
         opts = _Options(int(iq_bf16), int(das_tile), int(decode_tc))
-        self._h = lib().cutb_plan_create(ctypes.byref(self.bp), ctypes.byref(opts))
+        self._L = lib()
+        self._h = self._L.cutb_plan_create(ctypes.byref(self.bp), ctypes.byref(opts))
         _check(self._h, "cutb_plan_create")
         self.iq_bf16 = bool(iq_bf16)
         self.raw_bytes = lib().cutb_plan_raw_bytes(self._h)
@@ -299,8 +300,9 @@ class Plan:
         self.volume_bytes = lib().cutb_plan_volume_bytes(self._h)
 
     def close(self):
+        # _L is bound at construction: at interpreter exit the module globals may be gone.
         if getattr(self, "_h", None):
-            lib().cutb_plan_destroy(self._h)
+            self._L.cutb_plan_destroy(self._h)
             self._h = None
 
     __del__ = close
@@ -383,14 +385,15 @@ class Batch:
         opts = None
         if das_tiles is not None:
             opts = (_Options * n)(*[_Options(0, int(t), 0) for t in das_tiles])
-        self._h = lib().cutb_batch_create(self._bps, opts, n)
+        self._L = lib()
+        self._h = self._L.cutb_batch_create(self._bps, opts, n)
         _check(self._h, "cutb_batch_create")
         self.n = n
         self.shapes = [bp.volume_shape for bp in params]
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().cutb_batch_destroy(self._h)
+            self._L.cutb_batch_destroy(self._h)
             self._h = None
 
     __del__ = close
