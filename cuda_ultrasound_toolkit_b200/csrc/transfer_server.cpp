@@ -82,15 +82,7 @@ struct cutb_server {
         CUTB_REQUIRE(base.size() < 80 && base.find('/') == std::string::npos, CUTB_ERR_INVALID_ARGUMENT,
                      "Transfer name '%s' must be shorter than 80 characters, without '/'.", base.c_str());
         data_bytes = bytes ? (size_t)bytes : (size_t)DATA_SMEM_SIZE;
-        data_name = "/" + base + DATA_SMEM_SUFFIX;
-        params_name = "/" + base + PARAMETERS_SMEM_SUFFIX;
         sock_name = base + COMMAND_SOCKET_SUFFIX;
-        data = (uint8_t*)create_segment(data_name, data_bytes);
-        CUTB_REQUIRE(data, CUTB_ERR_ALLOCATION, "Failed to set up data shared memory '%s' (%zu bytes): %s",
-                     data_name.c_str(), data_bytes, strerror(errno));
-        params = (SharedMemoryParams*)create_segment(params_name, sizeof(SharedMemoryParams));
-        CUTB_REQUIRE(params, CUTB_ERR_ALLOCATION, "Failed to set up parameter shared memory '%s': %s",
-                     params_name.c_str(), strerror(errno));
         listen_fd = socket(AF_UNIX, SOCK_SEQPACKET | SOCK_CLOEXEC, 0);
         CUTB_REQUIRE(listen_fd >= 0, CUTB_ERR_INVALID_ARGUMENT, "Failed to create the command socket: %s",
                      strerror(errno));
@@ -98,9 +90,23 @@ struct cutb_server {
         addr.sun_family = AF_UNIX;
         memcpy(addr.sun_path + 1, sock_name.data(), sock_name.size());
         const socklen_t len = (socklen_t)(offsetof(sockaddr_un, sun_path) + 1 + sock_name.size());
-        CUTB_REQUIRE(bind(listen_fd, (sockaddr*)&addr, len) == 0 && listen(listen_fd, 4) == 0,
-                     CUTB_ERR_INVALID_ARGUMENT, "Failed to set up command socket '%s': %s", sock_name.c_str(),
-                     strerror(errno));
+        // The socket name is the lock: a second server of the same name fails here, before it
+        // could replace the running server's segments.
+        if (bind(listen_fd, (sockaddr*)&addr, len) != 0 || listen(listen_fd, 4) != 0) {
+            const int e = errno;
+            set_error(CUTB_ERR_INVALID_ARGUMENT, "Failed to set up command socket '%s': %s", sock_name.c_str(),
+                      strerror(e));
+            return false;
+        }
+        // Named only now: the destructor removes the segments of these names.
+        data_name = "/" + base + DATA_SMEM_SUFFIX;
+        params_name = "/" + base + PARAMETERS_SMEM_SUFFIX;
+        data = (uint8_t*)create_segment(data_name, data_bytes);
+        CUTB_REQUIRE(data, CUTB_ERR_ALLOCATION, "Failed to set up data shared memory '%s' (%zu bytes): %s",
+                     data_name.c_str(), data_bytes, strerror(errno));
+        params = (SharedMemoryParams*)create_segment(params_name, sizeof(SharedMemoryParams));
+        CUTB_REQUIRE(params, CUTB_ERR_ALLOCATION, "Failed to set up parameter shared memory '%s': %s",
+                     params_name.c_str(), strerror(errno));
         return true;
     }
 

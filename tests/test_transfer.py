@@ -229,6 +229,17 @@ def test_builtin_handler_validation_without_gpu(T):
         c.close()
 
 
+def test_second_server_of_the_same_name_is_refused(T):
+    """The command socket name acts as the lock: a second server fails to start and leaves the
+    running server's shared memory in place."""
+    p = NccMotionParameters.make(frame_count=1, image_dims=(4, 4), motion_grid_dims=(1, 1))
+    with T.Server(T.NAME, 1 << 20, handler=_echo) as s:
+        s.start()
+        with pytest.raises(Exception):
+            T.Server(T.NAME, 1 << 20, handler=_echo)
+        assert T.motion_detect_f32(np.ones((1, 4, 4), np.float32), p)[0, 0, 0, 0] == 16
+
+
 def test_server_executable_starts_and_times_out(native):
     from cuda_ultrasound_toolkit_b200 import transfer
     name = "cutbt" + uuid.uuid4().hex[:10]
