@@ -177,6 +177,7 @@ DAS_CASES = [
     dict(focus_z=15e-3),                                # YZ_FOCUS
     dict(time_offset=2e-7),
     dict(z=(0.0, 60e-3)),                               # reaches z = 0 and the clamp at S-2
+    dict(z=(0.0, 60e-3), cf=1.0),                       # packed path: clamped and clamp-free stages, CF
     dict(readi=2, readi_id=1),
     dict(readi=4, readi_id=2, decode=EncodingMatrix.WALSH),
     dict(seq=SequenceId.FORCES),
