@@ -250,9 +250,38 @@ __device__ void corr_map_smem(const float* ssm, int sws, const float* tsm, int t
 
 // find_peaks_kernel (block_match_kernels.cu:8-61): the 32 largest of the first 2048 map values
 // (-1 past the end of the map), larger value first, equal values by lower index; written to
-// cand[0..31] as map indices. Every thread keeps its 8 keys sorted; 32 rounds of a block maximum,
-// the owner of each winner drops it.
-__device__ void select_candidates(const float* cmap, int n, int* cand, unsigned long long (*wbuf)[kWarps])
+// cand[0..31] as map indices. Keys are (radix order of the value, complement of the index), so the
+// order is that of a 64-bit maximum and every key is unique. Two levels, one block barrier: each
+// warp draws the 32 largest of its 256 keys (every thread keeps its 8 sorted and the owner of each
+// warp maximum drops it), then warp 0 draws the 32 largest of the 8 sorted lists.
+__device__ __forceinline__ unsigned long long warp_max64(unsigned long long v)
+{
+    // high words first, then low words among the lanes that hold the highest high word
+    const uint32_t hi = (uint32_t)(v >> 32), lo = (uint32_t)v;
+    const uint32_t mh = __reduce_max_sync(0xffffffffu, hi);
+    const uint32_t ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
+    return ((unsigned long long)mh << 32) | ml;
+}
+
+// 32 rounds: the warp maximum of the lanes' heads, dropped by its owner. Lane r receives the r-th.
+template <int K>
+__device__ __forceinline__ unsigned long long warp_top32(unsigned long long (&key)[K])
+{
+    const int lane = threadIdx.x & 31;
+    unsigned long long mine = 0;
+    for (int round = 0; round < kCandidates; ++round) {
+        const unsigned long long m = warp_max64(key[0]);
+        if (key[0] == m) {
+#pragma unroll
+            for (int i = 0; i + 1 < K; ++i) key[i] = key[i + 1];
+            key[K - 1] = 0ull;
+        }
+        if (lane == round) mine = m;
+    }
+    return mine;
+}
+
+__device__ void select_candidates(const float* cmap, int n, int* cand, unsigned long long* lists)
 {
     unsigned long long key[kPerThread];
 #pragma unroll
@@ -271,25 +300,15 @@ __device__ void select_candidates(const float* cmap, int n, int* cand, unsigned 
                 key[j - 1] = t;
             }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // 64-bit maximum from two 32-bit warp reductions: high words, then low words among the
-    // lanes holding the highest high word.
-    auto warp_max = [](unsigned long long v) {
-        const uint32_t hi = (uint32_t)(v >> 32), lo = (uint32_t)v;
-        const uint32_t mh = __reduce_max_sync(0xffffffffu, hi);
-        const uint32_t ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
-        return ((unsigned long long)mh << 32) | ml;
-    };
-    for (int round = 0; round < kCandidates; ++round) {
-        const unsigned long long m = warp_max(key[0]);
-        if (lane == 0) wbuf[round & 1][warp] = m;
-        __syncthreads();
-        const unsigned long long best = warp_max(wbuf[round & 1][lane & (kWarps - 1)]);
-        if (key[0] == best) {  // keys are unique (index part)
+    lists[warp * kCandidates + lane] = warp_top32(key);  // each list sorted, largest first
+    __syncthreads();
+    if (warp == 0) {
+        // lane l holds entries 8 (l % 4) .. 8 (l % 4) + 7 of warp (l / 4)'s list: already sorted
+        unsigned long long k[kPerThread];
 #pragma unroll
-            for (int i = 0; i + 1 < kPerThread; ++i) key[i] = key[i + 1];
-            key[kPerThread - 1] = 0ull;
-        }
-        if (threadIdx.x == 0) cand[round] = (int)(0xFFFFFFFFu - (uint32_t)best);
+        for (int i = 0; i < kPerThread; ++i) k[i] = lists[lane * kPerThread + i];
+        const unsigned long long best = warp_top32(k);
+        cand[lane] = (int)(0xFFFFFFFFu - (uint32_t)best);
     }
     __syncthreads();
 }
@@ -385,7 +404,7 @@ __global__ void __launch_bounds__(kThreads, 3) block_match_kernel(MotionArgs a)
 {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ double red[kWarps];
-    __shared__ unsigned long long wbuf[2][kWarps];
+    __shared__ unsigned long long lists[kWarps * kCandidates];
     __shared__ int cand[kCandidates];
 
     const int cell = blockIdx.x, pair = blockIdx.y;
@@ -434,7 +453,7 @@ __global__ void __launch_bounds__(kThreads, 3) block_match_kernel(MotionArgs a)
             ssm[y * L.sws + x] = x < w.sw ? __ldg(S + (size_t)y * a.W + x) - shift : 0.f;
     __syncthreads();
     corr_map_smem(ssm, L.sws, tsm, tws, w.tw, w.th, cw, ch, tvar, h1, h2, cmap);
-    select_candidates(cmap, cw * ch, cand, wbuf);
+    select_candidates(cmap, cw * ch, cand, lists);
     if (threadIdx.x < 32)
         test_candidates(cmap, cw, ch, cand, w.tl - w.sl, w.tt - w.st, a,
                         reinterpret_cast<float4*>(a.maps) + ((size_t)f * a.gx * a.gy + cell));
