@@ -38,6 +38,14 @@ struct DecCfg {
     static constexpr uint32_t kTmemCols = 2u * MT * N;  // hi and lo accumulators per M tile
     static_assert(kTmemCols <= 256, "two CTAs per SM");
     static constexpr uint32_t kLboB = (N / 16) * 128;    // stride of 8-transmit groups in a plane
+    // Epilogue staging per warp: 32 output rows of SC samples, rows padded by 4 floats (stride
+    // 4 mod 8 words: conflict-free writes, whole-row reads); 32 columns when two CTAs still fit
+    // beside the 64 KB encoding image of T > 128, else 16.
+    static constexpr int SC = MT == 1 ? 32 : 16;
+    static constexpr int kStageRow = SC + 4;
+    static constexpr int kLanesPerRow = SC / 4;            // float4 per staged row
+    static constexpr int kRowsPerStore = 32 / kLanesPerRow;
+    static constexpr uint32_t kStageBytes = 4u * 32 * kStageRow * sizeof(float);
 };
 
 template <int MT, int N, int OSTRIDE>
@@ -53,6 +61,7 @@ __global__ void __launch_bounds__(kThreads, 2) decode_tc_kernel(const int16_t* _
     uint8_t* A = smem;
     uint8_t* Bhi = smem + a_bytes;
     uint8_t* Blo = Bhi + (uint32_t)T * N;
+    float* stage = reinterpret_cast<float*>(Blo + (uint32_t)T * N);  // 4 warps x 32 rows x kStageRow
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int c = blockIdx.y;
@@ -130,22 +139,55 @@ __global__ void __launch_bounds__(kThreads, 2) decode_tc_kernel(const int16_t* _
         const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
         for (int m = 0; m < MT; ++m) {
             const int tp = m * 128 + 32 * warp + lane;  // output row
+            if (OSTRIDE == 1) {
+                // A lane holds one output row, but a store instruction should cover few rows:
+                // SC samples of the warp's 32 rows go through its staging tile and leave as
+                // whole-row segments (4 rows x 128 bytes or 8 rows x 64 bytes per store
+                // instruction) instead of 32 rows x 16 bytes.
+                float* tile = stage + warp * (32 * C::kStageRow);
 #pragma unroll 1
-            for (int q = 0; q < N / 8; ++q) {
-                int h[8], l[8];
-                tmem_ld8_i32(lane_addr + (2 * m) * N + 8 * q, h);
-                tmem_ld8_i32(lane_addr + (2 * m + 1) * N + 8 * q, l);
-                tmem_wait_ld();
-                const int s = s0 + 8 * q;
-                if (tp >= T || s >= (int)a.S) continue;
-                float f[8];
+                for (int qs = 0; qs < N / C::SC; ++qs) {
+                    const int s = s0 + C::SC * qs;
 #pragma unroll
-                for (int i = 0; i < 8; ++i) f[i] = __fmul_rn((float)(h[i] * 256 + l[i]), a.alpha);
-                float* o = a.out + (((size_t)tp * a.C + c) * a.S + s) * OSTRIDE;
-                if (OSTRIDE == 1) {
-                    reinterpret_cast<float4*>(o)[0] = make_float4(f[0], f[1], f[2], f[3]);
-                    reinterpret_cast<float4*>(o)[1] = make_float4(f[4], f[5], f[6], f[7]);
-                } else {
+                    for (int qq = 0; qq < C::SC / 8; ++qq) {
+                        int h[8], l[8];
+                        tmem_ld8_i32(lane_addr + (2 * m) * N + C::SC * qs + 8 * qq, h);
+                        tmem_ld8_i32(lane_addr + (2 * m + 1) * N + C::SC * qs + 8 * qq, l);
+                        tmem_wait_ld();
+                        float f[8];
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) f[i] = __fmul_rn((float)(h[i] * 256 + l[i]), a.alpha);
+                        float4* row = reinterpret_cast<float4*>(tile + lane * C::kStageRow + 8 * qq);
+                        row[0] = make_float4(f[0], f[1], f[2], f[3]);
+                        row[1] = make_float4(f[4], f[5], f[6], f[7]);
+                    }
+                    __syncwarp();
+                    const int col = 4 * (lane % C::kLanesPerRow);
+                    if (s + col < (int)a.S) {  // S is a multiple of 8: a float4 is all in or out
+#pragma unroll
+                        for (int k = 0; k < 32 / C::kRowsPerStore; ++k) {
+                            const int rr = C::kRowsPerStore * k + lane / C::kLanesPerRow;
+                            const int tr = m * 128 + 32 * warp + rr;
+                            if (tr < T)
+                                *reinterpret_cast<float4*>(a.out + ((size_t)tr * a.C + c) * a.S + s + col) =
+                                    *reinterpret_cast<const float4*>(tile + rr * C::kStageRow + col);
+                        }
+                    }
+                    __syncwarp();
+                }
+            } else {
+#pragma unroll 1
+                for (int q = 0; q < N / 8; ++q) {
+                    int h[8], l[8];
+                    tmem_ld8_i32(lane_addr + (2 * m) * N + 8 * q, h);
+                    tmem_ld8_i32(lane_addr + (2 * m + 1) * N + 8 * q, l);
+                    tmem_wait_ld();
+                    const int s = s0 + 8 * q;
+                    if (tp >= T || s >= (int)a.S) continue;
+                    float f[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) f[i] = __fmul_rn((float)(h[i] * 256 + l[i]), a.alpha);
+                    float* o = a.out + (((size_t)tp * a.C + c) * a.S + s) * OSTRIDE;
 #pragma unroll
                     for (int i = 0; i < 8; i += 2)
                         reinterpret_cast<float4*>(o)[i / 2] = make_float4(f[i], 0.f, f[i + 1], 0.f);
@@ -162,7 +204,7 @@ template <int MT, int N, int OSTRIDE>
 bool launch_tc(const int16_t* raw, const int8_t* image, const DecodeTcArgs& a, cudaStream_t st)
 {
     auto k = decode_tc_kernel<MT, N, OSTRIDE>;
-    const uint32_t used = (uint32_t)MT * 128 * a.T + 2u * a.T * N;
+    const uint32_t used = (uint32_t)MT * 128 * a.T + 2u * a.T * N + DecCfg<MT, N>::kStageBytes;
     // at most two CTAs per SM, so that their TMEM (2 x 256 columns) always fits
     const uint32_t smem = used > 80u * 1024 ? used : 80u * 1024;
     CUTB_CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
