@@ -8,13 +8,17 @@
 // |H . x_hi| <= 128 T and |H . x_lo| <= 255 T, so for T <= 256 the combination is exact in int32
 // and, scaled by fl32(1/T), bit-identical to the FWHT path and to upstream's FP32 GEMM.
 //
-// A CTA decodes one receive channel c over N samples: A = H (M = 128 output rows per tile, K =
-// transmits, K-major, rows beyond T zero) comes from a prebuilt canonical image by one bulk
-// copy; the threads load the int16 tile [T][N] of raw channel map[c] with 16-byte loads, split
-// it into a signed-high and an unsigned-low byte plane written in the MN-major operand layout
-// (16 samples x 8 transmits per core matrix), and one thread issues the MMAs: per 32 transmits
-// one for each plane into its own TMEM accumulator. The epilogue combines hi and lo, scales and
-// stores rows t' of [T][C][S].
+// Persistent CTAs (two per SM, 256 TMEM columns each) walk the (receive channel c, N-sample
+// tile) items. A = H (M = 128 output rows per tile, K = transmits, K-major, rows beyond T zero)
+// comes from a prebuilt canonical image by one bulk copy per CTA. Per item the threads load the
+// int16 tile [T][N] of raw channel map[c] with 16-byte loads, split it into a signed-high and an
+// unsigned-low byte plane in the MN-major operand layout (16 samples x 8 transmits per core
+// matrix), and one thread issues the MMAs: per 32 transmits one for each plane into its own TMEM
+// accumulator. Planes and accumulators are double-buffered, so an item's MMAs and the next
+// item's loads run during the previous item's epilogue, which combines hi and lo, scales, and
+// stores rows t' of [T][C][S] through a per-warp staging tile as whole-row segments.
+#include <algorithm>
+
 #include "common.cuh"
 #include "stages.h"
 #include "tc05.cuh"
@@ -35,40 +39,54 @@ __host__ __device__ constexpr size_t a_offset(int T, int m, int r, int k)
 
 template <int MT, int N>
 struct DecCfg {
-    static constexpr uint32_t kTmemCols = 2u * MT * N;  // hi and lo accumulators per M tile
+    static constexpr uint32_t kSetCols = 2u * MT * N;     // hi and lo accumulators per M tile
+    static constexpr uint32_t kTmemCols = 2u * kSetCols;  // two sets: one tile's MMAs, the last one's epilogue
     static_assert(kTmemCols <= 256, "two CTAs per SM");
-    static constexpr uint32_t kLboB = (N / 16) * 128;    // stride of 8-transmit groups in a plane
+    static constexpr uint32_t kLboB = (N / 16) * 128;     // stride of 8-transmit groups in a plane
+    static constexpr int kMaxVec = 8;                     // 16-byte raw vectors per thread and tile
+    static_assert((MT * 128) * N / 8 / kThreads <= kMaxVec, "tile load per thread");
     // Epilogue staging per warp: 32 output rows of SC samples, rows padded by 4 floats (stride
     // 4 mod 8 words: conflict-free writes, whole-row reads); 32 columns when two CTAs still fit
     // beside the 64 KB encoding image of T > 128, else 16.
     static constexpr int SC = MT == 1 ? 32 : 16;
+    static_assert(N % SC == 0, "staged columns");
     static constexpr int kStageRow = SC + 4;
     static constexpr int kLanesPerRow = SC / 4;            // float4 per staged row
     static constexpr int kRowsPerStore = 32 / kLanesPerRow;
     static constexpr uint32_t kStageBytes = 4u * 32 * kStageRow * sizeof(float);
 };
 
+// Persistent CTAs (two per SM) over (channel, sample-tile) items, item = c * ntiles + tile. Per
+// iteration j:
+//   1. the prefetched raw vectors of item j become the byte planes of buffer j % 2;
+//   2. one thread issues item j's MMAs into TMEM set j % 2 and commits them;
+//   3. the raw vectors of item j + 1 are loaded (in flight during step 4);
+//   4. item j - 1's accumulators (set (j - 1) % 2) are combined, scaled and stored.
+// Buffer and set j % 2 are rewritten in iteration j + 2, after step 4 of iteration j + 1 waited
+// for their MMAs and the barrier of step 1 ordered every TMEM read before the next MMAs. All
+// waits are bounded; a wait that gives up sets bit 2 of the status word.
 template <int MT, int N, int OSTRIDE>
 __global__ void __launch_bounds__(kThreads, 2) decode_tc_kernel(const int16_t* __restrict__ raw,
                                                                 const int8_t* __restrict__ a_image, DecodeTcArgs a)
 {
     using C = DecCfg<MT, N>;
     extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ uint64_t a_full, mma_done;
+    __shared__ uint64_t a_full, mma_done[2];
     __shared__ uint32_t tmem_base_s;
     const int T = (int)a.T;
     const uint32_t a_bytes = (uint32_t)MT * 128 * T;
+    const uint32_t plane = (uint32_t)T * N;
     uint8_t* A = smem;
-    uint8_t* Bhi = smem + a_bytes;
-    uint8_t* Blo = Bhi + (uint32_t)T * N;
-    float* stage = reinterpret_cast<float*>(Blo + (uint32_t)T * N);  // 4 warps x 32 rows x kStageRow
+    uint8_t* planes = smem + a_bytes;  // buffer b: hi at 2 b plane, lo at (2 b + 1) plane
+    float* stage = reinterpret_cast<float*>(planes + 4 * plane);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int c = blockIdx.y;
-    const int s0 = blockIdx.x * N;
+    const int ntiles = (int)((a.S + N - 1) / N);
+    const long long items = (long long)a.C * ntiles;
     if (tid == 0) {
         mbar_init(&a_full, 1);
-        mbar_init(&mma_done, 1);
+        mbar_init(&mma_done[0], 1);
+        mbar_init(&mma_done[1], 1);
         fence_mbar_init();
     }
     if (warp == 0) {
@@ -84,61 +102,47 @@ __global__ void __launch_bounds__(kThreads, 2) decode_tc_kernel(const int16_t* _
         bulk_load(A, a_image, a_bytes, &a_full);
     }
 
-    // Raw tile -> signed-high and unsigned-low byte planes (MN-major: 16 samples x 8 transmits).
-    const int16_t* src = raw + (size_t)a.map[c] * a.R0;
     constexpr int kVecPerRow = N / 8;
-    for (int v = tid; v < T * kVecPerRow; v += kThreads) {
-        const int t = v / kVecPerRow, j = v % kVecPerRow;
-        const int s = s0 + 8 * j;
-        uint4 x = make_uint4(0, 0, 0, 0);
-        if (s < (int)a.S) x = __ldcs(reinterpret_cast<const uint4*>(src + (size_t)t * a.S + s));
-        const uint32_t w[4] = {x.x, x.y, x.z, x.w};
-        uint32_t hi[2], lo[2];
+    const int nvec = T * kVecPerRow;
+    uint4 x[C::kMaxVec];
+    auto load = [&](long long item) {
+        const int c = (int)(item / ntiles), s0 = (int)(item % ntiles) * N;
+        const int16_t* src = raw + (size_t)a.map[c] * a.R0;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            // bytes of samples 4h..4h+3: low bytes and high bytes of the four int16 values
-            const uint32_t p = w[2 * h], q = w[2 * h + 1];
-            lo[h] = __byte_perm(p, q, 0x6420);
-            hi[h] = __byte_perm(p, q, 0x7531);
+        for (int k = 0; k < C::kMaxVec; ++k) {
+            const int v = tid + k * kThreads;
+            x[k] = make_uint4(0, 0, 0, 0);
+            if (v < nvec) {
+                const int t = v / kVecPerRow, s = s0 + 8 * (v % kVecPerRow);
+                if (s < (int)a.S) x[k] = __ldcs(reinterpret_cast<const uint4*>(src + (size_t)t * a.S + s));
+            }
         }
-        const uint32_t off = (t / 8) * C::kLboB + ((8 * j) / 16) * 128 + (t % 8) * 16 + (8 * j) % 16;
-        *reinterpret_cast<uint2*>(Bhi + off) = make_uint2(hi[0], hi[1]);
-        *reinterpret_cast<uint2*>(Blo + off) = make_uint2(lo[0], lo[1]);
-    }
-    fence_proxy_async_shared();
-    __syncthreads();
-
-    int ok_local = 1;
-    if (tid == 0) {
-        if (!mbar_wait(&a_full, 0)) {
-            if (a.status) atomicOr(a.status, 2);
-            ok_local = 0;
-        } else {
-            fence_after_sync();
-            constexpr uint32_t id_hi = idesc_i8(128, N, true, true, false, true);
-            constexpr uint32_t id_lo = idesc_i8(128, N, true, false, false, true);
-            const uint32_t sa = saddr(A), shi = saddr(Bhi), slo = saddr(Blo);
-            const uint32_t sbo_a = (uint32_t)(T / 16) * 128;
-            for (int m = 0; m < MT; ++m)
-                for (int ks = 0; ks < T / 32; ++ks) {
-                    const uint64_t ad = smem_desc(sa + m * 128 * T + ks * 256, 128, sbo_a);
-                    const uint64_t bh = smem_desc(shi + ks * 4 * C::kLboB, C::kLboB, 128);
-                    const uint64_t bl = smem_desc(slo + ks * 4 * C::kLboB, C::kLboB, 128);
-                    mma_i8(tmem + (2 * m) * N, ad, bh, id_hi, ks > 0);
-                    mma_i8(tmem + (2 * m + 1) * N, ad, bl, id_lo, ks > 0);
-                }
+    };
+    auto split = [&](int b) {
+        uint8_t* Bhi = planes + 2 * b * plane;
+        uint8_t* Blo = Bhi + plane;
+#pragma unroll
+        for (int k = 0; k < C::kMaxVec; ++k) {
+            const int v = tid + k * kThreads;
+            if (v >= nvec) continue;
+            const int t = v / kVecPerRow, j = v % kVecPerRow;
+            const uint32_t w[4] = {x[k].x, x[k].y, x[k].z, x[k].w};
+            uint32_t hi[2], lo[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                // bytes of samples 4h..4h+3: low bytes and high bytes of the four int16 values
+                lo[h] = __byte_perm(w[2 * h], w[2 * h + 1], 0x6420);
+                hi[h] = __byte_perm(w[2 * h], w[2 * h + 1], 0x7531);
+            }
+            const uint32_t off = (t / 8) * C::kLboB + ((8 * j) / 16) * 128 + (t % 8) * 16 + (8 * j) % 16;
+            *reinterpret_cast<uint2*>(Bhi + off) = make_uint2(hi[0], hi[1]);
+            *reinterpret_cast<uint2*>(Blo + off) = make_uint2(lo[0], lo[1]);
         }
-        mma_commit(&mma_done);
-    }
-    __syncwarp();
-    const bool ok = __all_sync(0xffffffffu, mbar_wait(&mma_done, 0)) && __shfl_sync(0xffffffffu, ok_local, 0);
-    fence_after_sync();
-    if (!ok) {
-        if (lane == 0 && a.status) atomicOr(a.status, 2);
-    } else {
-        const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
+    };
+    auto epilogue = [&](long long item, int set) {
+        const int c = (int)(item / ntiles), s0 = (int)(item % ntiles) * N;
+        const uint32_t lane_addr = tmem + set * C::kSetCols + ((uint32_t)(32 * warp) << 16);
         for (int m = 0; m < MT; ++m) {
-            const int tp = m * 128 + 32 * warp + lane;  // output row
             if (OSTRIDE == 1) {
                 // A lane holds one output row, but a store instruction should cover few rows:
                 // SC samples of the warp's 32 rows go through its staging tile and leave as
@@ -169,13 +173,14 @@ __global__ void __launch_bounds__(kThreads, 2) decode_tc_kernel(const int16_t* _
                             const int rr = C::kRowsPerStore * k + lane / C::kLanesPerRow;
                             const int tr = m * 128 + 32 * warp + rr;
                             if (tr < T)
-                                *reinterpret_cast<float4*>(a.out + ((size_t)tr * a.C + c) * a.S + s + col) =
-                                    *reinterpret_cast<const float4*>(tile + rr * C::kStageRow + col);
+                                __stcs(reinterpret_cast<float4*>(a.out + ((size_t)tr * a.C + c) * a.S + s + col),
+                                       *reinterpret_cast<const float4*>(tile + rr * C::kStageRow + col));
                         }
                     }
                     __syncwarp();
                 }
             } else {
+                const int tp = m * 128 + 32 * warp + lane;  // output row
 #pragma unroll 1
                 for (int q = 0; q < N / 8; ++q) {
                     int h[8], l[8];
@@ -194,8 +199,65 @@ __global__ void __launch_bounds__(kThreads, 2) decode_tc_kernel(const int16_t* _
                 }
             }
         }
+    };
+
+    long long item = blockIdx.x;
+    bool ok = true;
+    if (item < items) load(item);
+    if (tid == 0 && !mbar_wait(&a_full, 0)) ok = false;
+    ok = __syncthreads_and(ok);
+    int j = 0;
+    for (; ok && item < items; item += gridDim.x, ++j) {
+        const int b = j & 1;
+        split(b);
+        fence_proxy_async_shared();
+        fence_before_sync();
+        __syncthreads();
+        fence_after_sync();
+        if (tid == 0) {
+            constexpr uint32_t id_hi = idesc_i8(128, N, true, true, false, true);
+            constexpr uint32_t id_lo = idesc_i8(128, N, true, false, false, true);
+            const uint32_t sa = saddr(A), shi = saddr(planes + 2 * b * plane), slo = shi + plane;
+            const uint32_t sbo_a = (uint32_t)(T / 16) * 128;
+            const uint32_t d = tmem + b * C::kSetCols;
+            for (int m = 0; m < MT; ++m)
+                for (int ks = 0; ks < T / 32; ++ks) {
+                    const uint64_t ad = smem_desc(sa + m * 128 * T + ks * 256, 128, sbo_a);
+                    const uint64_t bh = smem_desc(shi + ks * 4 * C::kLboB, C::kLboB, 128);
+                    const uint64_t bl = smem_desc(slo + ks * 4 * C::kLboB, C::kLboB, 128);
+                    mma_i8(d + (2 * m) * N, ad, bh, id_hi, ks > 0);
+                    mma_i8(d + (2 * m + 1) * N, ad, bl, id_lo, ks > 0);
+                }
+            mma_commit(&mma_done[b]);
+        }
+        if (item + gridDim.x < items) load(item + gridDim.x);
+        if (j > 0) {
+            const int pb = (j - 1) & 1;
+            __syncwarp();
+            if (!__all_sync(0xffffffffu, mbar_wait(&mma_done[pb], ((j - 1) >> 1) & 1))) ok = false;
+            fence_after_sync();
+            if (ok) epilogue(item - gridDim.x, pb);
+            fence_before_sync();
+        }
+        ok = __syncthreads_and(ok);
     }
-    fence_before_sync();
+    if (ok && j > 0) {  // the last item's accumulators
+        const int pb = (j - 1) & 1;
+        if (!__all_sync(0xffffffffu, mbar_wait(&mma_done[pb], ((j - 1) >> 1) & 1))) ok = false;
+        fence_after_sync();
+        if (ok) epilogue(item - gridDim.x, pb);
+        fence_before_sync();
+    }
+    ok = __syncthreads_and(ok);
+    if (!ok) {
+        if (tid == 0 && a.status) atomicOr(a.status, 2);
+        // let MMAs and copies in flight finish (bounded) before TMEM and shared memory are released
+        if (tid == 0) {
+            mbar_wait(&a_full, 0);
+            mbar_wait(&mma_done[0], 0), mbar_wait(&mma_done[0], 1);
+            mbar_wait(&mma_done[1], 0), mbar_wait(&mma_done[1], 1);
+        }
+    }
     __syncthreads();
     if (warp == 0) tmem_dealloc(tmem, C::kTmemCols);
 }
@@ -204,11 +266,15 @@ template <int MT, int N, int OSTRIDE>
 bool launch_tc(const int16_t* raw, const int8_t* image, const DecodeTcArgs& a, cudaStream_t st)
 {
     auto k = decode_tc_kernel<MT, N, OSTRIDE>;
-    const uint32_t used = (uint32_t)MT * 128 * a.T + 2u * a.T * N + DecCfg<MT, N>::kStageBytes;
+    const uint32_t used = (uint32_t)MT * 128 * a.T + 4u * a.T * N + DecCfg<MT, N>::kStageBytes;
     // at most two CTAs per SM, so that their TMEM (2 x 256 columns) always fits
     const uint32_t smem = used > 80u * 1024 ? used : 80u * 1024;
     CUTB_CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const dim3 grid((a.S + N - 1) / N, a.C);
+    int dev = 0, sms = 148;
+    CUTB_CUDA_OK(cudaGetDevice(&dev));
+    CUTB_CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const long long items = (long long)a.C * ((a.S + N - 1) / N);
+    const unsigned grid = (unsigned)std::min<long long>(items, 2ll * sms);
     k<<<grid, kThreads, smem, st>>>(raw, image, a);
     CUTB_CUDA_OK(cudaGetLastError());
     return true;
@@ -243,8 +309,8 @@ bool launch_decode_tc(const DecodeTcArgs& a, const int8_t* image, const void* ra
                  CUTB_ERR_INVALID_ARGUMENT, "Tensor-core decode needs 16-byte aligned buffers.");
     const int16_t* r = (const int16_t*)raw;
     if (a.T > 128)
-        return out_stride == 1 ? launch_tc<2, 64, 1>(r, image, a, st) : launch_tc<2, 64, 2>(r, image, a, st);
-    return out_stride == 1 ? launch_tc<1, 128, 1>(r, image, a, st) : launch_tc<1, 128, 2>(r, image, a, st);
+        return out_stride == 1 ? launch_tc<2, 32, 1>(r, image, a, st) : launch_tc<2, 32, 2>(r, image, a, st);
+    return out_stride == 1 ? launch_tc<1, 64, 1>(r, image, a, st) : launch_tc<1, 64, 2>(r, image, a, st);
 }
 
 }  // namespace cutb
