@@ -171,15 +171,16 @@ struct StageMeta {
     int t, g, c0, nq;
 };
 
-// Shared memory: NS raw windows per row (TMA destination) and one buffer of cubic
-// coefficients per row: A[i] = (a, b), B[i] = (c, d) with value(t) = a + t (b + t (c + t d))
-// on [i, i + 1] (complex a..d), split so each is one 16-byte load.
-template <class IQ, bool CUBIC>
+// Shared memory: NS raw windows per row (TMA destination) and, for NC > 0, one buffer of
+// interpolation coefficients per row. Cubic (NC = 2): A[i] = (a, b), B[i] = (c, d) with
+// value(t) = a + t (b + t (c + t d)) on [i, i + 1] (complex a..d), split so each is one 16-byte
+// load. Linear (NC = 1): A[i] = (p[i], p[i + 1] - p[i]).
+template <class IQ, int NC>
 struct alignas(128) Smem {
     IQ raw[kStages][kRows][kWinMax];
-    float4 coefA[CUBIC ? kRows : 1][CUBIC ? kWinMax : 1];
-    float4 coefB[CUBIC ? kRows : 1][CUBIC ? kWinMax : 1];
-    RowMeta rowc[CUBIC ? kRows : 1];  // metadata of the rows whose coefficients are built
+    float4 coefA[NC >= 1 ? kRows : 1][NC >= 1 ? kWinMax : 1];
+    float4 coefB[NC == 2 ? kRows : 1][NC == 2 ? kWinMax : 1];
+    RowMeta rowc[NC >= 1 ? kRows : 1];  // metadata of the rows whose coefficients are built
     RowMeta row[kStages][kRows];
     StageMeta stage[kStages];
     RowMeta next_row[kSlots][kRows];    // precomputed metadata of upcoming stages (ring)
@@ -189,6 +190,11 @@ struct alignas(128) Smem {
     int abort;
     int tx_reach_bits;
 };
+
+// Coefficient arrays staged per row: cubic always 2; linear 1 where the packed row pass runs
+// (HERCULES without apodization), else 0 (the taps are read from the raw windows).
+template <int SEQ, bool CUBIC, bool APO>
+constexpr int coef_arrays() { return CUBIC ? 2 : (SEQ == HERCULES && !APO ? 1 : 0); }
 
 struct Tile {
     double cx, cy, cz;  // tile centre (FP64)
@@ -252,8 +258,8 @@ __device__ __forceinline__ StageMeta stage_meta(const DasArgs& a, const StageId&
 
 // Window bounds and metadata of row q of stage `id` into batch slot `slot` (one thread per
 // row; all threads of the CTA share the work of a batch of stages).
-template <int SEQ, class IQ, bool CUBIC>
-__device__ void compute_row(Smem<IQ, CUBIC>& sm, int slot, const StageId& id, int q, const DasArgs& a,
+template <int SEQ, class IQ, int NC>
+__device__ void compute_row(Smem<IQ, NC>& sm, int slot, const StageId& id, int q, const DasArgs& a,
                             const Tile& tile)
 {
     constexpr bool HERC = SEQ == HERCULES;
@@ -329,8 +335,8 @@ __device__ void compute_row(Smem<IQ, CUBIC>& sm, int slot, const StageId& id, in
 }
 
 // Metadata of stages first .. first+kBatch-1 (all threads; a barrier must follow).
-template <int SEQ, class IQ, bool CUBIC>
-__device__ __forceinline__ void compute_batch(Smem<IQ, CUBIC>& sm, int first, int nstages, int nchunks,
+template <int SEQ, class IQ, int NC>
+__device__ __forceinline__ void compute_batch(Smem<IQ, NC>& sm, int first, int nstages, int nchunks,
                                               const DasArgs& a, const Tile& tile)
 {
     for (int i = threadIdx.x; i < kBatch * kRows; i += kThreads) {
@@ -340,8 +346,8 @@ __device__ __forceinline__ void compute_batch(Smem<IQ, CUBIC>& sm, int first, in
 }
 
 // Issue stage k into buffer b from its precomputed metadata: lane q of one warp per row.
-template <class IQ, bool CUBIC>
-__device__ __forceinline__ void issue_row(Smem<IQ, CUBIC>& sm, int b, int k, int q, const DasArgs& a,
+template <class IQ, int NC>
+__device__ __forceinline__ void issue_row(Smem<IQ, NC>& sm, int b, int k, int q, const DasArgs& a,
                                           const IQ* __restrict__ iq)
 {
     const int slot = k % kSlots;
@@ -370,13 +376,21 @@ __device__ __forceinline__ float path_offset(float delta, float d0, float d0sq, 
 }
 
 // Cubic coefficients of every staged interval of stage buffer b (all threads).
-template <class IQ>
-__device__ __forceinline__ void build_coefficients(Smem<IQ, true>& sm, int b, int nq)
+template <class IQ, int NC>
+__device__ __forceinline__ void build_coefficients(Smem<IQ, NC>& sm, int b, int nq)
 {
     if (threadIdx.x < nq) sm.rowc[threadIdx.x] = sm.row[b][threadIdx.x];
     for (int q = 0; q < nq; ++q) {
         const int len = sm.row[b][q].len;
         const IQ* p = &sm.raw[b][q][0];
+        if constexpr (NC == 1) {
+            // linear: value(t) = p0 + t (p1 - p0), the operations of the scalar staged pass
+            for (int i = 1 + threadIdx.x; i <= len - 3; i += kThreads) {
+                const float2 p0 = to_f2(p[i]), p1 = to_f2(p[i + 1]);
+                sm.coefA[q][i] = make_float4(p0.x, p0.y, p1.x - p0.x, p1.y - p0.y);
+            }
+            continue;
+        } else {
         for (int i = 1 + threadIdx.x; i <= len - 3; i += kThreads) {
             const float2 pm1 = to_f2(p[i - 1]), p0 = to_f2(p[i]), p1 = to_f2(p[i + 1]), p2 = to_f2(p[i + 2]);
             float4 A, B;
@@ -391,13 +405,14 @@ __device__ __forceinline__ void build_coefficients(Smem<IQ, true>& sm, int b, in
             sm.coefA[q][i] = A;
             sm.coefB[q][i] = B;
         }
+        }
     }
 }
 
 // Accumulates one row into the thread's voxels. STAGED: from shared memory (coefficients
 // for cubic, raw taps for linear); otherwise from the global row with guarded taps.
-template <int SEQ, bool CUBIC, bool CF, bool APO, bool STAGED, class IQ, bool CUBIC_SM>
-__device__ __forceinline__ void row_pass(const DasArgs& a, const Smem<IQ, CUBIC_SM>& sm, const RowMeta* rows, int b,
+template <int SEQ, bool CUBIC, bool CF, bool APO, bool STAGED, class IQ, int NCS>
+__device__ __forceinline__ void row_pass(const DasArgs& a, const Smem<IQ, NCS>& sm, const RowMeta* rows, int b,
                                          int qi, const IQ* grow, const StageMeta& st, float dxe, const float (&sq)[kVpt],
                                          const float (&txs)[kVpt], const float (&vzv)[kVpt], float vx, float a2,
                                          float2 (&total)[kVpt], float (&inc)[kVpt])
@@ -510,8 +525,8 @@ __device__ __forceinline__ float rsqrt_approx(float x)
 // element the operations are those of row_pass: -(exdx + sq) negates the rounded sum exactly,
 // so d0^2 - (-delta) = d0^2 + delta. Only the coherence energy is kept as (re^2, im^2) partial
 // sums, added at the end.
-template <bool CF, bool CLAMP, class IQ>
-__device__ __forceinline__ void row_pass_packed(const Smem<IQ, true>& sm, const RowMeta* rows, int qi, float dxe,
+template <bool CF, bool CLAMP, class IQ, int NC>
+__device__ __forceinline__ void row_pass_packed(const Smem<IQ, NC>& sm, const RowMeta* rows, int qi, float dxe,
                                                 float spm, f2x ww, const f2x (&sq2)[kVpt / 2],
                                                 const f2x (&txs2)[kVpt / 2], f2x (&tot2)[kVpt], f2x (&inc2)[kVpt])
 {
@@ -524,7 +539,7 @@ __device__ __forceinline__ void row_pass_packed(const Smem<IQ, true>& sm, const 
     const f2x magic2 = pk(kMagic, kMagic);
     const float loc = m.loclamp, hic = m.hiclamp;
     const float4* cA = sm.coefA[qi];
-    const float4* cB = sm.coefB[qi];
+    const float4* cB = sm.coefB[NC == 2 ? qi : 0];
 #pragma unroll
     for (int p = 0; p < kVpt / 2; ++p) {
         const f2x nd = sub2(nexdx2, sq2[p]);  // -delta
@@ -554,8 +569,14 @@ __device__ __forceinline__ void row_pass_packed(const Smem<IQ, true>& sm, const 
         for (int h = 0; h < 2; ++h) {
             const int i = h ? i1 : i0;
             const f2x tt = h ? pk(t1, t1) : pk(t0, t0);
-            const float4 A = cA[i], B = cB[i];
-            const f2x v = fma2(fma2(fma2(pk(B.z, B.w), tt, pk(B.x, B.y)), tt, pk(A.z, A.w)), tt, pk(A.x, A.y));
+            f2x v;
+            if constexpr (NC == 2) {
+                const float4 A = cA[i], B = cB[i];
+                v = fma2(fma2(fma2(pk(B.z, B.w), tt, pk(B.x, B.y)), tt, pk(A.z, A.w)), tt, pk(A.x, A.y));
+            } else {
+                const float4 A = cA[i];
+                v = fma2(pk(A.z, A.w), tt, pk(A.x, A.y));
+            }
             tot2[2 * p + h] = fma2(ww, v, tot2[2 * p + h]);
             if (CF) inc2[2 * p + h] = fma2(v, v, inc2[2 * p + h]);
         }
@@ -581,8 +602,10 @@ struct Layout {
 // kernel (a in parameter space) and by the persistent batch kernel (a in its parameter table).
 template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT>
 __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __restrict__ vol, const DasArgs& a,
-                                         Smem<IQ, CUBIC>& sm, int bx, int by, int bz, int split)
+                                         Smem<IQ, coef_arrays<SEQ, CUBIC, APO>()>& sm, int bx, int by, int bz,
+                                         int split)
 {
+    constexpr int NC = coef_arrays<SEQ, CUBIC, APO>();
     constexpr bool HERC = SEQ == HERCULES;
     using L = Layout<SEQ, SHORT>;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -649,8 +672,10 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
 #pragma unroll
     for (int v = 0; v < kVpt; ++v) qz[v] = fmaf(two_cz, dz[v], fmaf(dxe, dxe, fmaf(dye, dye, dz[v] * dz[v])));
 
-    // HERCULES + cubic without apodization accumulates on packed FP32x2 (row_pass_packed).
-    constexpr bool PACKED = HERC && CUBIC && !APO;
+    // HERCULES without apodization accumulates on packed FP32x2 (row_pass_packed), from cubic or
+    // linear coefficients.
+    constexpr bool PACKED = HERC && !APO;
+    static_assert(!PACKED || NC > 0, "the packed pass reads coefficients");
     float2 total[kVpt];
     float inc[kVpt];
     f2x tot2[PACKED ? kVpt : 1], inc2[PACKED ? kVpt : 1], txs2[PACKED ? kVpt / 2 : 1];
@@ -690,14 +715,14 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
         if (next < nstages && (next - k_begin) % kBatch == 0)
             compute_batch<SEQ>(sm, next, nstages, nchunks, a, tile);
         int all_staged = 1;
-        if constexpr (CUBIC) {
+        if constexpr (NC > 0) {
             build_coefficients(sm, b, st.nq);
             all_staged = __syncthreads_and(threadIdx.x >= st.nq || sm.row[b][threadIdx.x].len > 0);
             // The raw buffer is free once transformed: refill it while this stage computes.
             if (warp == 0 && lane < kRows && next < nstages && !sm.abort) issue_row(sm, b, next, lane, a, iq);
         }
-        const RowMeta* rows = CUBIC ? sm.rowc : sm.row[b];
-        if (!CUBIC)
+        const RowMeta* rows = NC > 0 ? sm.rowc : sm.row[b];
+        if (NC == 0)
             for (int q = 0; q < st.nq; ++q) all_staged &= rows[q].len > 0;
         // Per-stage, per-voxel part of d^2 - d0^2 (receive path) and the FORCES transmit offset.
         float sq[kVpt], tsh[kVpt];
@@ -763,7 +788,7 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
         }
         __syncthreads();
         if (sm.abort) break;
-        if (!CUBIC && warp == 0 && lane < kRows && next < nstages) issue_row(sm, b, next, lane, a, iq);
+        if (NC == 0 && warp == 0 && lane < kRows && next < nstages) issue_row(sm, b, next, lane, a, iq);
     }
     if (sm.abort) {
         // Let every copy already issued land before the CTA's shared memory is released.
@@ -813,7 +838,7 @@ __global__ void __launch_bounds__(kThreads, 3)
 das_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    auto& sm = *reinterpret_cast<Smem<IQ, CUBIC>*>(smem_raw);
+    auto& sm = *reinterpret_cast<Smem<IQ, coef_arrays<SEQ, CUBIC, APO>()>*>(smem_raw);
     using L = Layout<SEQ, SHORT>;
     int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
     int split = 0;
@@ -836,7 +861,7 @@ __global__ void __launch_bounds__(kThreads, 3)
 das_batch_kernel(const DasBatchParams P, const int2* __restrict__ items, int nitems, int* __restrict__ counter)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    auto& sm = *reinterpret_cast<Smem<IQ, CUBIC>*>(smem_raw);
+    auto& sm = *reinterpret_cast<Smem<IQ, coef_arrays<SEQ, CUBIC, APO>()>*>(smem_raw);
     using L = Layout<SEQ, SHORT>;
     __shared__ int item_s;
     for (;;) {
@@ -865,7 +890,7 @@ bool launch_das_t(const DasArgs& a, const void* iq, void* volume, cudaStream_t s
     if (a.tiles) grid = dim3(a.ntiles, a.splits > 1 ? a.splits : 1, 1);
     CUTB_REQUIRE(grid.y <= 65535 && grid.z <= 65535, CUTB_ERR_UNSUPPORTED, "Output grid too large.");
     auto kern = das_kernel<SEQ, CUBIC, CF, APO, IQ, SHORT>;
-    const size_t smem = sizeof(Smem<IQ, CUBIC>);
+    const size_t smem = sizeof(Smem<IQ, coef_arrays<SEQ, CUBIC, APO>()>);
     static bool configured = false;
     if (!configured) {
         CUTB_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1044,7 +1069,7 @@ bool launch_batch_t(const DasBatchParams* P, const int2* items, int nitems, int*
                     cudaStream_t st)
 {
     auto kern = das_batch_kernel<HERCULES, CUBIC, CF, APO, IQ, SHORT>;
-    const size_t smem = sizeof(Smem<IQ, CUBIC>);
+    const size_t smem = sizeof(Smem<IQ, coef_arrays<HERCULES, CUBIC, APO>()>);
     if (grid <= 0) {
         CUTB_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         CUTB_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kern, kThreads, smem));
