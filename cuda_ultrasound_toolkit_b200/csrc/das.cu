@@ -46,6 +46,7 @@ constexpr int kVpt = 8;           // voxels per thread (along z)
 constexpr int kRows = 8;          // rows (channels) per stage
 constexpr int kStages = 3;        // raw stage buffers in flight
 constexpr int kWinMax = 136;      // samples per staged window
+constexpr int kWinShort = 88;     // ... for the double-buffered short-window form
 constexpr int kBatch = 8;         // stages whose window metadata is computed together
 constexpr int kSlots = 2 * kBatch;  // metadata ring: a batch never overwrites a stage still being issued
 constexpr float kPi = 3.141592654f;  // value of CUDART_PI_F used upstream
@@ -175,19 +176,27 @@ struct StageMeta {
 // interpolation coefficients per row. Cubic (NC = 2): A[i] = (a, b), B[i] = (c, d) with
 // value(t) = a + t (b + t (c + t d)) on [i, i + 1] (complex a..d), split so each is one 16-byte
 // load. Linear (NC = 1): A[i] = (p[i], p[i + 1] - p[i]).
-template <class IQ, int NC>
+//
+// DB: two coefficient buffers (stage j builds into buffer j % 2), so that a stage needs one
+// block barrier instead of two; it fits three CTAs per SM only with shorter windows (kWinShort).
+template <class IQ, int NC, bool DB = false>
 struct alignas(128) Smem {
-    IQ raw[kStages][kRows][kWinMax];
-    float4 coefA[NC >= 1 ? kRows : 1][NC >= 1 ? kWinMax : 1];
-    float4 coefB[NC == 2 ? kRows : 1][NC == 2 ? kWinMax : 1];
-    RowMeta rowc[NC >= 1 ? kRows : 1];  // metadata of the rows whose coefficients are built
+    static constexpr int kWin = DB ? kWinShort : kWinMax;
+    static constexpr int kCB = DB ? 2 : 1;
+    IQ raw[kStages][kRows][kWin];
+    float4 coefA[NC >= 1 ? kCB : 1][NC >= 1 ? kRows : 1][NC >= 1 ? kWin : 1];
+    float4 coefB[NC == 2 ? kCB : 1][NC == 2 ? kRows : 1][NC == 2 ? kWin : 1];
+    RowMeta rowc[NC >= 1 ? kCB : 1][NC >= 1 ? kRows : 1];  // metadata of the rows whose coefficients are built
     RowMeta row[kStages][kRows];
     StageMeta stage[kStages];
     RowMeta next_row[kSlots][kRows];    // precomputed metadata of upcoming stages (ring)
     StageMeta next_stage[kSlots];
     int next_bytes[kSlots][kRows];
     uint64_t full[kStages];
-    int abort;
+    // Abort flag per stage parity: set by a thread whose bounded wait for stage j gave up, before
+    // stage j's barrier, and read by every thread after it. A thread one stage ahead writes the
+    // other slot, so all threads leave the stage loop at the same stage.
+    int abort[2];
     int tx_reach_bits;
 };
 
@@ -258,8 +267,8 @@ __device__ __forceinline__ StageMeta stage_meta(const DasArgs& a, const StageId&
 
 // Window bounds and metadata of row q of stage `id` into batch slot `slot` (one thread per
 // row; all threads of the CTA share the work of a batch of stages).
-template <int SEQ, class IQ, int NC>
-__device__ void compute_row(Smem<IQ, NC>& sm, int slot, const StageId& id, int q, const DasArgs& a,
+template <int SEQ, class IQ, int NC, bool DB>
+__device__ void compute_row(Smem<IQ, NC, DB>& sm, int slot, const StageId& id, int q, const DasArgs& a,
                             const Tile& tile)
 {
     constexpr bool HERC = SEQ == HERCULES;
@@ -315,7 +324,7 @@ __device__ void compute_row(Smem<IQ, NC>& sm, int slot, const StageId& id, int q
         m.loclamp = (float)(1 - lo);
         m.hiclamp = (float)(a.S - 2 - lo);
         m.len = 0;
-        if (len + SA <= kWinMax) {
+        if (len + SA <= Smem<IQ, NC, DB>::kWin) {
             m.len = len;
             m.loclamp = fmaxf(m.loclamp, 1.f);
             m.hiclamp = fminf(m.hiclamp, (float)(len - 3));
@@ -335,8 +344,8 @@ __device__ void compute_row(Smem<IQ, NC>& sm, int slot, const StageId& id, int q
 }
 
 // Metadata of stages first .. first+kBatch-1 (all threads; a barrier must follow).
-template <int SEQ, class IQ, int NC>
-__device__ __forceinline__ void compute_batch(Smem<IQ, NC>& sm, int first, int nstages, int nchunks,
+template <int SEQ, class IQ, int NC, bool DB>
+__device__ __forceinline__ void compute_batch(Smem<IQ, NC, DB>& sm, int first, int nstages, int nchunks,
                                               const DasArgs& a, const Tile& tile)
 {
     for (int i = threadIdx.x; i < kBatch * kRows; i += kThreads) {
@@ -346,8 +355,8 @@ __device__ __forceinline__ void compute_batch(Smem<IQ, NC>& sm, int first, int n
 }
 
 // Issue stage k into buffer b from its precomputed metadata: lane q of one warp per row.
-template <class IQ, int NC>
-__device__ __forceinline__ void issue_row(Smem<IQ, NC>& sm, int b, int k, int q, const DasArgs& a,
+template <class IQ, int NC, bool DB>
+__device__ __forceinline__ void issue_row(Smem<IQ, NC, DB>& sm, int b, int k, int q, const DasArgs& a,
                                           const IQ* __restrict__ iq)
 {
     const int slot = k % kSlots;
@@ -376,10 +385,10 @@ __device__ __forceinline__ float path_offset(float delta, float d0, float d0sq, 
 }
 
 // Cubic coefficients of every staged interval of stage buffer b (all threads).
-template <class IQ, int NC>
-__device__ __forceinline__ void build_coefficients(Smem<IQ, NC>& sm, int b, int nq)
+template <class IQ, int NC, bool DB>
+__device__ __forceinline__ void build_coefficients(Smem<IQ, NC, DB>& sm, int b, int nq, int cb)
 {
-    if (threadIdx.x < nq) sm.rowc[threadIdx.x] = sm.row[b][threadIdx.x];
+    if (threadIdx.x < nq) sm.rowc[cb][threadIdx.x] = sm.row[b][threadIdx.x];
     for (int q = 0; q < nq; ++q) {
         const int len = sm.row[b][q].len;
         const IQ* p = &sm.raw[b][q][0];
@@ -387,7 +396,7 @@ __device__ __forceinline__ void build_coefficients(Smem<IQ, NC>& sm, int b, int 
             // linear: value(t) = p0 + t (p1 - p0), the operations of the scalar staged pass
             for (int i = 1 + threadIdx.x; i <= len - 3; i += kThreads) {
                 const float2 p0 = to_f2(p[i]), p1 = to_f2(p[i + 1]);
-                sm.coefA[q][i] = make_float4(p0.x, p0.y, p1.x - p0.x, p1.y - p0.y);
+                sm.coefA[cb][q][i] = make_float4(p0.x, p0.y, p1.x - p0.x, p1.y - p0.y);
             }
             continue;
         } else {
@@ -402,8 +411,8 @@ __device__ __forceinline__ void build_coefficients(Smem<IQ, NC>& sm, int b, int 
             B.y = fmaf(-0.5f, p2.y, fmaf(2.f, p1.y, fmaf(-2.5f, p0.y, pm1.y)));
             B.z = fmaf(0.5f, p2.x - pm1.x, 1.5f * (p0.x - p1.x));
             B.w = fmaf(0.5f, p2.y - pm1.y, 1.5f * (p0.y - p1.y));
-            sm.coefA[q][i] = A;
-            sm.coefB[q][i] = B;
+            sm.coefA[cb][q][i] = A;
+            sm.coefB[cb][q][i] = B;
         }
         }
     }
@@ -411,8 +420,8 @@ __device__ __forceinline__ void build_coefficients(Smem<IQ, NC>& sm, int b, int 
 
 // Accumulates one row into the thread's voxels. STAGED: from shared memory (coefficients
 // for cubic, raw taps for linear); otherwise from the global row with guarded taps.
-template <int SEQ, bool CUBIC, bool CF, bool APO, bool STAGED, class IQ, int NCS>
-__device__ __forceinline__ void row_pass(const DasArgs& a, const Smem<IQ, NCS>& sm, const RowMeta* rows, int b,
+template <int SEQ, bool CUBIC, bool CF, bool APO, bool STAGED, class IQ, int NCS, bool DB>
+__device__ __forceinline__ void row_pass(const DasArgs& a, const Smem<IQ, NCS, DB>& sm, const RowMeta* rows, int b,
                                          int qi, const IQ* grow, const StageMeta& st, float dxe, const float (&sq)[kVpt],
                                          const float (&txs)[kVpt], const float (&vzv)[kVpt], float vx, float a2,
                                          float2 (&total)[kVpt], float (&inc)[kVpt])
@@ -451,12 +460,13 @@ __device__ __forceinline__ void row_pass(const DasArgs& a, const Smem<IQ, NCS>& 
         float idx = fmaf(corr, a.spm, base + txs[v]);
         idx = fminf(fmaxf(idx, loc), hic);
         float2 val;
-        if (STAGED) {
+        if constexpr (STAGED) {
             const float f = __fadd_rd(idx, kMagic);
             const int i = __float_as_int(f) - __float_as_int(kMagic);
             const float t = idx - (f - kMagic);
             if constexpr (CUBIC) {
-                const float4 A = sm.coefA[qi][i], B = sm.coefB[qi][i];
+                static_assert(!DB, "the scalar staged pass reads the single coefficient buffer");
+                const float4 A = sm.coefA[0][qi][i], B = sm.coefB[0][qi][i];
                 val.x = fmaf(fmaf(fmaf(B.z, t, B.x), t, A.z), t, A.x);
                 val.y = fmaf(fmaf(fmaf(B.w, t, B.y), t, A.w), t, A.y);
             } else {
@@ -525,8 +535,8 @@ __device__ __forceinline__ float rsqrt_approx(float x)
 // element the operations are those of row_pass: -(exdx + sq) negates the rounded sum exactly,
 // so d0^2 - (-delta) = d0^2 + delta. Only the coherence energy is kept as (re^2, im^2) partial
 // sums, added at the end.
-template <bool CF, bool CLAMP, class IQ, int NC>
-__device__ __forceinline__ void row_pass_packed(const Smem<IQ, NC>& sm, const RowMeta* rows, int qi, float dxe,
+template <bool CF, bool CLAMP, class IQ, int NC, bool DB>
+__device__ __forceinline__ void row_pass_packed(const Smem<IQ, NC, DB>& sm, int cb, const RowMeta* rows, int qi, float dxe,
                                                 float spm, f2x ww, const f2x (&sq2)[kVpt / 2],
                                                 const f2x (&txs2)[kVpt / 2], f2x (&tot2)[kVpt], f2x (&inc2)[kVpt])
 {
@@ -538,8 +548,8 @@ __device__ __forceinline__ void row_pass_packed(const Smem<IQ, NC>& sm, const Ro
     const f2x base2 = pk(m.base, m.base), spm2 = pk(spm, spm), mhalf2 = pk(-0.5f, -0.5f);
     const f2x magic2 = pk(kMagic, kMagic);
     const float loc = m.loclamp, hic = m.hiclamp;
-    const float4* cA = sm.coefA[qi];
-    const float4* cB = sm.coefB[NC == 2 ? qi : 0];
+    const float4* cA = sm.coefA[cb][qi];
+    const float4* cB = sm.coefB[NC == 2 ? cb : 0][NC == 2 ? qi : 0];
 #pragma unroll
     for (int p = 0; p < kVpt / 2; ++p) {
         const f2x nd = sub2(nexdx2, sq2[p]);  // -delta
@@ -600,12 +610,13 @@ struct Layout {
 
 // One tile (bx, by, bz) of the volume, stage slice `split` of a.splits. Called by the grid
 // kernel (a in parameter space) and by the persistent batch kernel (a in its parameter table).
-template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT>
+template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT, bool DB = false>
 __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __restrict__ vol, const DasArgs& a,
-                                         Smem<IQ, coef_arrays<SEQ, CUBIC, APO>()>& sm, int bx, int by, int bz,
+                                         Smem<IQ, coef_arrays<SEQ, CUBIC, APO>(), DB>& sm, int bx, int by, int bz,
                                          int split)
 {
     constexpr int NC = coef_arrays<SEQ, CUBIC, APO>();
+    static_assert(!DB || NC > 0, "two coefficient buffers need coefficients");
     constexpr bool HERC = SEQ == HERCULES;
     using L = Layout<SEQ, SHORT>;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -652,7 +663,7 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
     // depth, so it is measured rather than bounded). FORCES: the transmit path is 1-Lipschitz.
     if (threadIdx.x == 0) {
         sm.tx_reach_bits = 0;
-        sm.abort = 0;
+        sm.abort[0] = sm.abort[1] = 0;
         for (int b = 0; b < kStages; ++b) mbar_init(&sm.full[b], kRows);
         fence_mbar_init();
     }
@@ -707,7 +718,7 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
         const int j = k - k_begin;  // local stage number: buffer and barrier phase
         const int b = j % kStages;
         if (!mbar_wait_bounded(&sm.full[b], (unsigned)(j / kStages) & 1u)) {
-            sm.abort = 1;
+            sm.abort[j & 1] = 1;
             atomicOr(a.status, 1);
         }
         const StageMeta st = sm.stage[b];
@@ -715,13 +726,20 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
         if (next < nstages && (next - k_begin) % kBatch == 0)
             compute_batch<SEQ>(sm, next, nstages, nchunks, a, tile);
         int all_staged = 1;
+        // DB: stage j builds into coefficient buffer j % 2, last read by stage j - 2's rows, which
+        // every warp finished before the barrier below in stage j - 1; so the end-of-stage
+        // barrier is not needed. A warp can then be one stage ahead of another, and touches
+        // only that stage's buffers: coefficients j + 1 (other parity), raw stage and mbarrier
+        // (j + 1) % kStages, metadata ring slots of stages j + kStages + 1 onwards.
+        const int cb = DB ? (j & 1) : 0;
         if constexpr (NC > 0) {
-            build_coefficients(sm, b, st.nq);
+            build_coefficients(sm, b, st.nq, cb);
             all_staged = __syncthreads_and(threadIdx.x >= st.nq || sm.row[b][threadIdx.x].len > 0);
+            if (DB && sm.abort[j & 1]) break;
             // The raw buffer is free once transformed: refill it while this stage computes.
-            if (warp == 0 && lane < kRows && next < nstages && !sm.abort) issue_row(sm, b, next, lane, a, iq);
+            if (warp == 0 && lane < kRows && next < nstages && !sm.abort[j & 1]) issue_row(sm, b, next, lane, a, iq);
         }
-        const RowMeta* rows = NC > 0 ? sm.rowc : sm.row[b];
+        const RowMeta* rows = NC > 0 ? sm.rowc[cb] : sm.row[b];
         if (NC == 0)
             for (int q = 0; q < st.nq; ++q) all_staged &= rows[q].len > 0;
         // Per-stage, per-voxel part of d^2 - d0^2 (receive path) and the FORCES transmit offset.
@@ -753,19 +771,19 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
             if (unclamped && st.nq == kRows) {
 #pragma unroll
                 for (int qi = 0; qi < kRows; ++qi)
-                    row_pass_packed<CF, false>(sm, rows, qi, dxe, a.spm, ww, sq2, txs2, tot2, inc2);
+                    row_pass_packed<CF, false>(sm, cb, rows, qi, dxe, a.spm, ww, sq2, txs2, tot2, inc2);
             } else if (unclamped) {
 #pragma unroll 4
                 for (int qi = 0; qi < st.nq; ++qi)
-                    row_pass_packed<CF, false>(sm, rows, qi, dxe, a.spm, ww, sq2, txs2, tot2, inc2);
+                    row_pass_packed<CF, false>(sm, cb, rows, qi, dxe, a.spm, ww, sq2, txs2, tot2, inc2);
             } else if (all_staged) {
 #pragma unroll 4
                 for (int qi = 0; qi < st.nq; ++qi)
-                    row_pass_packed<CF, true>(sm, rows, qi, dxe, a.spm, ww, sq2, txs2, tot2, inc2);
+                    row_pass_packed<CF, true>(sm, cb, rows, qi, dxe, a.spm, ww, sq2, txs2, tot2, inc2);
             } else {
                 for (int qi = 0; qi < st.nq; ++qi) {
                     if (rows[qi].len > 0)
-                        row_pass_packed<CF, true>(sm, rows, qi, dxe, a.spm, ww, sq2, txs2, tot2, inc2);
+                        row_pass_packed<CF, true>(sm, cb, rows, qi, dxe, a.spm, ww, sq2, txs2, tot2, inc2);
                     else
                         row_pass<SEQ, CUBIC, CF, APO, false>(a, sm, rows, b, qi, grow0 + (size_t)qi * a.S, st, dxe, sq,
                                                              tsh, vzv, vx, a2, total, inc);
@@ -786,11 +804,13 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
                                                          vzv, vx, a2, total, inc);
             }
         }
-        __syncthreads();
-        if (sm.abort) break;
+        if constexpr (!DB) {
+            __syncthreads();
+            if (sm.abort[j & 1]) break;
+        }
         if (NC == 0 && warp == 0 && lane < kRows && next < nstages) issue_row(sm, b, next, lane, a, iq);
     }
-    if (sm.abort) {
+    if (sm.abort[0] | sm.abort[1]) {
         // Let every copy already issued land before the CTA's shared memory is released.
         for (int k = 0; k < kStages; ++k) mbar_wait_bounded(&sm.full[k], 0), mbar_wait_bounded(&sm.full[k], 1);
         return;
@@ -833,12 +853,12 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
 
 // Whole grid: blockIdx.xyz is the tile. Tile list: blockIdx.x indexes a.tiles and blockIdx.y
 // is the slice of the stages (transmits x channel groups) this CTA sums.
-template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT>
+template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT, bool DB>
 __global__ void __launch_bounds__(kThreads, 3)
 das_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    auto& sm = *reinterpret_cast<Smem<IQ, coef_arrays<SEQ, CUBIC, APO>()>*>(smem_raw);
+    auto& sm = *reinterpret_cast<Smem<IQ, coef_arrays<SEQ, CUBIC, APO>(), DB>*>(smem_raw);
     using L = Layout<SEQ, SHORT>;
     int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
     int split = 0;
@@ -850,7 +870,7 @@ das_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
         bz = id / (nx * ny);
         split = blockIdx.y;
     }
-    das_tile<SEQ, CUBIC, CF, APO, IQ, SHORT>(iq, vol, a, sm, bx, by, bz, split);
+    das_tile<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>(iq, vol, a, sm, bx, by, bz, split);
 }
 
 // Persistent delay-and-sum over the tiles of many frames: CTAs take (frame, tile) work items,
@@ -875,22 +895,22 @@ das_batch_kernel(const DasBatchParams P, const int2* __restrict__ items, int nit
         das_tile<SEQ, CUBIC, CF, APO, IQ, SHORT>((const IQ*)f.iq, f.vol, f.a, sm, w.y % nx, (w.y / nx) % ny,
                                                  w.y / (nx * ny), 0);
         __syncthreads();
-        if (sm.abort) break;
+        if (sm.abort[0] | sm.abort[1]) break;
         if (threadIdx.x == 0)
             for (int b = 0; b < kStages; ++b) mbar_inval(&sm.full[b]);
         __syncthreads();
     }
 }
 
-template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT>
-bool launch_das_t(const DasArgs& a, const void* iq, void* volume, cudaStream_t st)
+template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT, bool DB>
+bool launch_das_k(const DasArgs& a, const void* iq, void* volume, cudaStream_t st)
 {
     using L = Layout<SEQ, SHORT>;
     dim3 grid(div_up(a.X, L::TX), div_up(a.Y, L::TY), div_up(a.Z, L::TZ));
     if (a.tiles) grid = dim3(a.ntiles, a.splits > 1 ? a.splits : 1, 1);
     CUTB_REQUIRE(grid.y <= 65535 && grid.z <= 65535, CUTB_ERR_UNSUPPORTED, "Output grid too large.");
-    auto kern = das_kernel<SEQ, CUBIC, CF, APO, IQ, SHORT>;
-    const size_t smem = sizeof(Smem<IQ, coef_arrays<SEQ, CUBIC, APO>()>);
+    auto kern = das_kernel<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>;
+    const size_t smem = sizeof(Smem<IQ, coef_arrays<SEQ, CUBIC, APO>(), DB>);
     static bool configured = false;
     if (!configured) {
         CUTB_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -899,6 +919,27 @@ bool launch_das_t(const DasArgs& a, const void* iq, void* volume, cudaStream_t s
     kern<<<grid, kThreads, smem, st>>>((const IQ*)iq, (float2*)volume, a);
     CUTB_CUDA_OK(cudaGetLastError());
     return true;
+}
+
+// True when the short tile's staged window (the bound of prefer_short_tile for its half
+// extents) fits the double-buffered form's kWinShort-sample buffers. Rows whose window still
+// does not fit are read from global memory, so this only selects the faster form.
+bool short_windows_fit(const DasArgs& a)
+{
+    using L = Layout<HERCULES, true>;
+    const double hx = 0.5 * (L::TX - 1) * std::fabs((double)a.res_x), hy = 0.5 * (L::TY - 1) * std::fabs((double)a.res_y);
+    const double hz = 0.5 * (L::TZ - 1) * std::fabs((double)a.res_z);
+    const double reach = std::sqrt(hx * hx + hy * hy + hz * hz) * (double)a.spm;
+    return 4.0 * reach + 8.0 <= (double)(kWinShort - 8);
+}
+
+template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT>
+bool launch_das_t(const DasArgs& a, const void* iq, void* volume, cudaStream_t st)
+{
+    // HERCULES, short tile, coefficients: one barrier per stage when the windows are short.
+    if constexpr (SEQ == HERCULES && SHORT && coef_arrays<SEQ, CUBIC, APO>() > 0 && !APO)
+        if (short_windows_fit(a)) return launch_das_k<SEQ, CUBIC, CF, APO, IQ, SHORT, true>(a, iq, volume, st);
+    return launch_das_k<SEQ, CUBIC, CF, APO, IQ, SHORT, false>(a, iq, volume, st);
 }
 
 // True when the 8 x 8 x 16 HERCULES tile is used. It is the default for volumes at least 8

@@ -213,7 +213,12 @@ def test_das_vs_fp64(torch, orc, case):
 TILE_CASES = [dict(), dict(cf=1.0, cubic=False), dict(focus_z=15e-3), dict(X=33, Y=3, Z=70),
               dict(z=(10e-3, 14e-3)), dict(z=(10e-3, 13e-3), cf=1.0, fn_rx=1.5),
               # staged windows with linear interpolation over many stages (C = 64 -> 8 per transmit)
-              dict(z=(10e-3, 14e-3), cubic=False, C=64, T=16), dict(z=(10e-3, 14e-3), cubic=False, cf=0.7, C=32)]
+              dict(z=(10e-3, 14e-3), cubic=False, C=64, T=16), dict(z=(10e-3, 14e-3), cubic=False, cf=0.7, C=32),
+              # fine grids: the 8x8x16 tile's window bound (4 reach + 8 samples) fits the 80 samples of the
+              # double-buffered form; X=25 sits just inside the bound (78.9), X=24 just outside (81.5)
+              dict(X=40, Z=48, z=(10e-3, 12e-3)), dict(X=40, Z=48, z=(10e-3, 12e-3), cubic=False, cf=0.7, C=64, T=16),
+              dict(X=40, Z=48, z=(0.0, 2e-3), cf=1.0), dict(X=44, Y=11, Z=35, z=(20e-3, 21.5e-3), time_offset=2e-7),
+              dict(X=25, Z=40, z=(10e-3, 13e-3)), dict(X=24, Z=40, z=(10e-3, 13e-3))]
 
 
 @pytest.mark.parametrize("tile", [1, 2], ids=["tile4x8x32", "tile8x8x16"])
