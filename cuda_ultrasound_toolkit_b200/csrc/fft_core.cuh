@@ -135,16 +135,40 @@ __host__ __device__ constexpr int pass_count(int logn) { return logn / 4 + (logn
 __host__ __device__ constexpr int pass_radix(int logn, int p) { return p < logn / 4 ? 16 : 1 << (logn % 4); }
 __host__ __device__ constexpr int pass_ns_log(int logn, int p) { return 4 * p; }  // log2 of points combined before pass p
 
-// Padded shared-memory index: one float of padding every 32 floats.
-__host__ __device__ __forceinline__ uint32_t spad(uint32_t i) { return i + (i >> 5); }
-__host__ __device__ constexpr uint32_t spad_size(uint32_t n) { return n + (n >> 5) + 1; }
+// Swizzled shared-memory index: the bank bits of i are XORed with S(b), b = i / 32,
+// S(b) = (b mod 16) + 16 * bit3(b). A warp's 32 stores of one register in the first pass
+// (i = 16 tau + r) and in the second (i = 256 (tau / 16) + tau mod 16 + 16 r) then hit 32
+// different banks, and a gather of 32 consecutive elements stays a permutation of one row
+// of banks.
+__host__ __device__ __forceinline__ uint32_t spad(uint32_t i) { return i ^ (((i >> 5) & 15u) | ((i >> 4) & 16u)); }
+__host__ __device__ constexpr uint32_t spad_size(uint32_t n) { return n; }
 
 // Butterflies of pass p for thread tau, reading and writing registers x[]. For the last
 // pass the results stay in registers (natural order); otherwise they are scattered to
 // the shared arrays sre/sim at their output positions. tw = exp(-2*pi*i*m/N), m < N.
+// Base twiddles of the radix-16 passes p > 0 of thread tau: wb[p] = {w^k, w^(4k)} with
+// w = exp(-2*pi*i/(ns*16)), k = tau mod ns; the 15 twiddles of the pass are products of these.
+template <int LOGN>
+struct BaseTwiddles {
+    cplx w[pass_count(LOGN) > 1 ? pass_count(LOGN) : 1][2];
+};
+template <int LOGN>
+__host__ __device__ __forceinline__ void load_base_twiddles(BaseTwiddles<LOGN>& wb, uint32_t tau,
+                                                            const cplx* __restrict__ tw)
+{
+#pragma unroll
+    for (int p = 1; p < pass_count(LOGN); ++p) {
+        if (pass_radix(LOGN, p) != 16) continue;
+        const int sh = LOGN - pass_ns_log(LOGN, p) - 4;
+        const uint32_t k = tau & ((1u << pass_ns_log(LOGN, p)) - 1);
+        wb.w[p][0] = tw[k << sh];
+        wb.w[p][1] = tw[(4 * k) << sh];
+    }
+}
+
 template <int LOGN, int P, int SIGN>
 __host__ __device__ __forceinline__ void fft_pass(cplx (&x)[16], uint32_t tau, const cplx* __restrict__ tw,
-                                                  float* sre, float* sim)
+                                                  float* sre, float* sim, const BaseTwiddles<LOGN>& wb)
 {
     constexpr int N = 1 << LOGN;
     constexpr int TPF = N / 16;
@@ -161,7 +185,24 @@ __host__ __device__ __forceinline__ void fft_pass(cplx (&x)[16], uint32_t tau, c
         cplx v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = x[u + r * B];
-        if constexpr (P > 0) {
+        if constexpr (P > 0 && R == 16) {
+            // w^(r k), r = 1..15, from two table entries w^k and w^(4k): w^(4a + b) = w^(4a) w^b,
+            // at most three rounded products deep.
+            cplx p[16];
+            p[1] = wb.w[P][0];
+            p[4] = wb.w[P][1];
+            if constexpr (SIGN > 0) p[1].y = -p[1].y, p[4].y = -p[4].y;
+            p[2] = cmul(p[1], p[1]);
+            p[3] = cmul(p[2], p[1]);
+            p[8] = cmul(p[4], p[4]);
+            p[12] = cmul(p[8], p[4]);
+#pragma unroll
+            for (int a4 = 4; a4 < 16; a4 += 4)
+#pragma unroll
+                for (int b = 1; b < 4; ++b) p[a4 + b] = cmul(p[a4], p[b]);
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[r] = cmul(v[r], p[r]);
+        } else if constexpr (P > 0) {
 #pragma unroll
             for (int r = 1; r < R; ++r) {
                 cplx w = tw[(r * k) << TW_SHIFT];
