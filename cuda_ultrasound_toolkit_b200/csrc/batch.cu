@@ -1,11 +1,17 @@
-// Batched beamforming of many frames of uneven size: every frame's front end (decode + Hilbert)
-// followed by ONE persistent delay-and-sum launch per kernel variant over all frames' tiles,
+// Batched beamforming of many frames of uneven size: every frame's front end (decode + Hilbert),
+// then the delay-and-sum of the frames that fill the GPU on their own as their own grid launches,
+// and ONE persistent delay-and-sum launch per kernel variant over the tiles of all smaller frames;
 // optionally captured once into a CUDA graph and replayed.
 //
 // Why: a small frame (64^3 voxels, 32 x 64 rows) fills a fraction of the 148 SMs and a stream of
 // such frames pays a launch and a tail per stage. The persistent kernel takes (frame, tile) work
 // items from one device counter, heaviest tiles first (longest-processing-time order), so the
 // GPU stays full until the last tile of the last frame; the graph removes per-launch host cost.
+// A frame with at least one full wave of tiles (SMs x resident CTAs) gains nothing from that and
+// runs the single-frame kernel, which reads its arguments from kernel parameters instead of a
+// table indexed at run time (the persistent kernel measured about 6 % slower per tile). The
+// delay-and-sum launches alternate between two streams forked from the batch's stream (parallel
+// branches in the graph), so one launch's tail overlaps the next launch's first wave.
 // Frames keep their own parameter blocks (dimensions, geometry, channel map, match filter);
 // frames with identical blocks share one plan (tables), each frame has its own buffers.
 #include <algorithm>
@@ -49,8 +55,9 @@ struct cutb_batch {
     std::vector<float*> decoded;
     std::vector<void*> iq;
     std::vector<Group> groups;
-    cudaStream_t own = nullptr;
-    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    std::vector<int> direct;  // frames whose delay-and-sum is a grid launch of its own
+    cudaStream_t own = nullptr, side[2] = {nullptr, nullptr};
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_fe = nullptr, ev_side[2] = {nullptr, nullptr};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     std::vector<const void*> g_raw;
@@ -62,6 +69,11 @@ struct cutb_batch {
         if (graph) cudaGraphDestroy(graph);
         if (ev_in) cudaEventDestroy(ev_in);
         if (ev_out) cudaEventDestroy(ev_out);
+        if (ev_fe) cudaEventDestroy(ev_fe);
+        for (int k = 0; k < 2; ++k) {
+            if (ev_side[k]) cudaEventDestroy(ev_side[k]);
+            if (side[k]) cudaStreamDestroy(side[k]);
+        }
         if (own) cudaStreamDestroy(own);
         for (auto& g : groups) {
             device_free(g.d_items);
@@ -75,6 +87,9 @@ struct cutb_batch {
     bool build(const CudaBeamformerParameters* bp, const cutb_options* opts, uint count)
     {
         n = (int)count;
+        int dev = 0, sms = 148;
+        CUTB_CUDA_OK(cudaGetDevice(&dev));
+        CUTB_CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         for (int i = 0; i < n; ++i) {
             int found = -1;
             for (size_t k = 0; k < plans.size(); ++k)
@@ -110,6 +125,13 @@ struct cutb_batch {
             iq.push_back(q);
             const DasArgs& a = p->das;
             const bool shrt = das_uses_short_tile(a);
+            int t[3], per_sm = 0;
+            das_grid_tiles(a, t);
+            if (!launch_das_batch(nullptr, nullptr, 0, nullptr, a, p->iq_bf16, shrt, 0, &per_sm, 0)) return false;
+            if ((long long)t[0] * t[1] * t[2] >= (long long)sms * std::max(per_sm, 1)) {
+                direct.push_back(i);
+                continue;
+            }
             Group* g = nullptr;
             for (auto& gg : groups)
                 if (same_group(gg, a, shrt, p->iq_bf16)) g = &gg;
@@ -122,9 +144,6 @@ struct cutb_batch {
             }
             g->frames.push_back(i);
         }
-        int dev = 0, sms = 148;
-        CUTB_CUDA_OK(cudaGetDevice(&dev));
-        CUTB_CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         for (auto& g : groups) {
             struct Item {
                 long long cost;
@@ -156,10 +175,16 @@ struct cutb_batch {
         CUTB_CUDA_OK(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
         CUTB_CUDA_OK(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
         CUTB_CUDA_OK(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
+        CUTB_CUDA_OK(cudaEventCreateWithFlags(&ev_fe, cudaEventDisableTiming));
+        for (int k = 0; k < 2; ++k) {
+            CUTB_CUDA_OK(cudaStreamCreateWithFlags(&side[k], cudaStreamNonBlocking));
+            CUTB_CUDA_OK(cudaEventCreateWithFlags(&ev_side[k], cudaEventDisableTiming));
+        }
         return true;
     }
 
-    // Every kernel of one run, on `st`, with no synchronisation (capturable).
+    // Every kernel of one run, ordered after `st` and before its end, with no host
+    // synchronisation (capturable: the side streams fork from and join back into `st`).
     bool enqueue(const void* const* raw, void* const* vol, cudaStream_t st)
     {
         for (int i = 0; i < n; ++i) {
@@ -167,17 +192,33 @@ struct cutb_batch {
             if (!p->fe.decode(raw[i], p->data_type, decoded[i], 1, st)) return false;
             if (!p->fe.hilbert(decoded[i], 1, iq[i], p->iq_bf16, st)) return false;
         }
+        CUTB_CUDA_OK(cudaEventRecord(ev_fe, st));
+        for (int k = 0; k < 2; ++k) CUTB_CUDA_OK(cudaStreamWaitEvent(side[k], ev_fe, 0));
+        int next = 0;
+        bool ok = true;
+        // Persistent launches first: the small frames' tiles then fill the direct launches' tails.
         for (auto& g : groups) {
+            if (!ok) break;
             for (int k = 0; k < (int)g.frames.size(); ++k) {
                 const int i = g.frames[k];
                 g.params->f[k] = DasFrame{plans[plan_of[i]]->das, iq[i], (float2*)vol[i]};
             }
-            CUTB_CUDA_OK(cudaMemsetAsync(g.d_counter, 0, sizeof(int), st));
-            if (!launch_das_batch(g.params.get(), g.d_items, (int)g.items.size(), g.d_counter, g.like, g.iq_bf16,
-                                  g.short_tile, g.grid, nullptr, st))
-                return false;
+            cudaStream_t s = side[next++ & 1];
+            ok = cudaMemsetAsync(g.d_counter, 0, sizeof(int), s) == cudaSuccess;
+            if (!ok) set_error(CUTB_ERR_CUDA, "Batch work counter reset failed.");
+            ok = ok && launch_das_batch(g.params.get(), g.d_items, (int)g.items.size(), g.d_counter, g.like,
+                                        g.iq_bf16, g.short_tile, g.grid, nullptr, s);
         }
-        return true;
+        for (size_t d = 0; ok && d < direct.size(); ++d) {
+            cutb_plan* p = plans[plan_of[direct[d]]];
+            ok = launch_das(p->das, iq[direct[d]], p->iq_bf16, vol[direct[d]], side[next++ & 1], nullptr);
+        }
+        // Join both side streams back into `st` even after a failure, so a capture stays joined.
+        for (int k = 0; k < 2; ++k) {
+            CUTB_CUDA_OK(cudaEventRecord(ev_side[k], side[k]));
+            CUTB_CUDA_OK(cudaStreamWaitEvent(st, ev_side[k], 0));
+        }
+        return ok;
     }
 
     bool run(const void* const* raw, void* const* vol, bool use_graph, cudaStream_t caller)
@@ -257,12 +298,16 @@ CUTB_API bool cutb_batch_check(cutb_batch* b, void* stream)
     return true;
 }
 
-// Kernels one run launches: decode and Hilbert per frame, one delay-and-sum per group.
+// Kernels one run launches: decode and Hilbert per frame, one delay-and-sum per group of small
+// frames and one per frame that fills the GPU on its own.
 CUTB_API int cutb_batch_launches_per_run(const cutb_batch* b)
 {
-    return b ? 2 * b->n + (int)b->groups.size() : 0;
+    return b ? 2 * b->n + (int)(b->groups.size() + b->direct.size()) : 0;
 }
 
-CUTB_API int cutb_batch_das_launches(const cutb_batch* b) { return b ? (int)b->groups.size() : 0; }
+CUTB_API int cutb_batch_das_launches(const cutb_batch* b)
+{
+    return b ? (int)(b->groups.size() + b->direct.size()) : 0;
+}
 
 }  // extern "C"

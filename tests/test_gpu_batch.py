@@ -76,6 +76,24 @@ def test_batch_mixed_tiles(frames):
         assert torch.equal(v, ref)
 
 
+def test_batch_direct_and_persistent_frames():
+    """A frame with a full wave of tiles (64 x 64 x 128: 512 tiles >= 148 SMs x 3 CTAs) runs its own
+    grid launch on a side stream, the small frames one persistent launch on the other; every
+    volume still equals the single-frame path, with and without the graph."""
+    specs = [dict(T=8, C=8, S=1024, X=64, Y=64, Z=128, scatterers=20, seed=11), SPECS[0], SPECS[3]]
+    fr = batched.make_frames(specs)
+    b = Batch([bp for _, bp in fr])
+    assert b.das_launches == 2
+    assert b.launches_per_run == 2 * len(fr) + 2
+    raws = [r for r, _ in fr]
+    ref = reference(fr)
+    for graph in (False, True, True):
+        vols = b.run(raws, graph=graph)
+        b.check()
+        for v, r in zip(vols, ref):
+            assert torch.equal(v, r)
+
+
 def test_tuner_choice_is_fastest_on_remeasure(tmp_path):
     spec = dict(T=32, C=64, S=2048, X=64, Y=64, Z=64, scatterers=50, seed=9)
     bp = batched.make_frames([spec])[0][1]
