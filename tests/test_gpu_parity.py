@@ -347,8 +347,11 @@ def test_bandpass_pipeline_vs_oracle(torch, orc):
     assert rel_l2(vol.ravel()[vox], orc.das(iq, bp, vox)) < TOL_DAS_RANDOM
 
 
-def test_das_bf16_storage(torch, orc):
-    bp = das_params(cf=1.0)
+@pytest.mark.parametrize("grid", [dict(), dict(X=40, Z=48, z=(10e-3, 12e-3))], ids=["coarse", "fine"])
+def test_das_bf16_storage(torch, orc, grid):
+    """BF16 analytic-signal storage; the fine grid's 8x8x16-tile window bound (51 samples) selects
+    the double-buffered-coefficient form."""
+    bp = das_params(cf=1.0, **grid)
     S, C, T = bp.dims
     iq = analytic_rows(orc, T, C, S, seed=9)
     plan = Plan(bp, iq_bf16=True)
