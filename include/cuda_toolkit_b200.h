@@ -110,9 +110,13 @@ CUTB_API bool cutb_das_tiles(cutb_plan* plan, const void* d_iq, void* d_volume, 
 
 /* ---- batched beamforming (no counterpart upstream) --------------------------------------------
  * Many frames of uneven size (each its own parameter block; HERCULES) beamformed together: every
- * frame's decode + Hilbert, then one persistent delay-and-sum launch per kernel variant that takes
- * (frame, tile) work items, heaviest first, from a device counter. Frames with identical blocks
- * and options share tables; every frame owns its intermediate buffers (allocated here).
+ * frame's decode + Hilbert, then the delay-and-sum: a frame with at least one full wave of tiles
+ * (SMs x resident CTAs) gets the single-frame kernel's grid launch; all smaller frames share one
+ * persistent launch per kernel variant that takes (frame, tile) work items, heaviest first, from a
+ * device counter. The delay-and-sum launches alternate between two internal streams so that one
+ * launch's tail overlaps the next. Frames with identical blocks and options share tables; every
+ * frame owns its intermediate buffers (allocated here). cutb_batch_das_launches counts the
+ * delay-and-sum launches of one run (persistent groups + direct frames).
  * cutb_batch_run: d_raw[i] -> d_volume[i] (complex64 [Z][Y][X]); with use_graph the whole run is
  * captured into a CUDA graph on the first call for a set of pointers and replayed afterwards.
  * Work runs on the batch's own stream, ordered after and before `stream`. */
