@@ -327,6 +327,11 @@ def run_ours(args, rank, world, local_rank):
             line["motion"] = motion_section()
         except Exception as exc:  # must not hide the plain pipeline's number
             line["motion"] = {"failed": str(exc)}
+    if args.sequences and world == 1:
+        try:
+            line["sequences"] = sequences_section()
+        except Exception as exc:  # must not hide the plain pipeline's number
+            line["sequences"] = {"failed": str(exc)}
     if args.transfer and world == 1:
         try:
             line["transfer"] = transfer_section()
@@ -583,6 +588,115 @@ def motion_section(reps=10, warmup=3):
     return out
 
 
+def _event_ms(fn, reps, warmup):
+    """Mean device time of fn() over reps calls (CUDA events on the current stream)."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def sequences_section(reps=5, warmup=3, seed=11):
+    """The other live sequences and the bandpass input, each on the GPU with the FP64 oracle timed
+    beside it on a bounded sample.
+
+    TPW (RCA_TPW, tilted plane waves in the x-z plane, IQ phase rotation) and UFORCES (sparse
+    transmit elements, focus at 30 mm): 64 transmits x 128 channels x 2048 samples of analytic
+    signal resident in HBM -> 256 x 1 x 512 (x, y, z), cubic + coherence factor; one thread per
+    voxel, y-invariant. Bandpass: 128 transmits x 128 channels of 4096 complex samples sent as
+    8192 interleaved int16 IQ values, Hadamard-encoded, 64-tap filter; exact decode of the raw
+    pairs, then demodulation + filter, both HBM-bound."""
+    import torch
+    from cuda_ultrasound_toolkit_b200 import Plan, synth
+    from cuda_ultrasound_toolkit_b200.params import SequenceId
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    rng = np.random.default_rng(seed)
+    out = {}
+    T, C, S, X, Z = 64, 128, 2048, 256, 512
+    for name in ("tpw", "uforces"):
+        w = synth.Workload(name, T, C, S, X, 1, Z, 0, cubic=True, cf=1.0)
+        bp = synth.make_params(w)
+        bp.tx_orientation = bp.rx_orientation  # x-z plane
+        bp.output_min_coordinate[0], bp.output_max_coordinate[0] = -C * synth.PITCH / 2, C * synth.PITCH / 2
+        bp.fn_rx = 1.0
+        if name == "tpw":
+            bp.das_shader_id = int(SequenceId.RCA_TPW)
+            for t, ang in enumerate(np.linspace(-0.25, 0.25, T)):
+                bp.foci[3 * t + 2] = float(ang)
+            used = T
+        else:
+            bp.das_shader_id = int(SequenceId.UFORCES)
+            bp.foci[2] = 30e-3
+            for t in range(T):
+                bp.sparse_elements[t] = 2 * t
+            used = T - 1  # transmit row 0 (the flash) is not summed
+        plan = Plan(bp)
+        iq = torch.complex(torch.randn(T, C, S, device="cuda"), torch.randn(T, C, S, device="cuda"))
+        vol = plan.empty_volume()
+        ms = _event_ms(lambda: plan.das(iq, out=vol), reps, warmup)
+        plan.check()
+        vtc = X * Z * used * C
+        n_vox = 256
+        vox = rng.choice(X * Z, n_vox, replace=False)
+        iq_h = iq.cpu().numpy().astype(np.complex128)
+        t0 = time.perf_counter()
+        ref = O.das(iq_h, bp, vox, threads)
+        cpu_s = time.perf_counter() - t0
+        got = vol.cpu().numpy().reshape(-1)[vox]
+        out[name] = {"workload": f"{T} tx x {C} ch x {S} samples -> {X} x 1 x {Z}, cubic + CF",
+                     "device_ms": ms, "vtc_per_s": vtc / ms * 1e3,
+                     "rel_l2_vs_fp64_sample": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
+                     "cpu_baseline": {"vtc_per_s": n_vox * used * C / cpu_s, "cores": threads, "kind": "port",
+                                      "sample": f"FP64 oracle, {n_vox} random voxels"}}
+        del iq, iq_h
+    T, C, S, ntaps = 128, 128, 4096, 64
+    w = synth.Workload("bandpass", T, C, S, 64, 64, 64, 0, cubic=True, cf=0.0)
+    bp = synth.make_params(w)
+    bp.rf_raw_dim[0] = 2 * T * S
+    bp.sample_type = 1
+    taps = synth.chirp_taps(ntaps)
+    bp.filter_length = ntaps
+    for i, v in enumerate(taps):
+        bp.rf_filter[i] = float(v)
+    plan = Plan(bp)
+    raw = torch.randint(-32768, 32768, (C, 2 * T * S), dtype=torch.int16, device="cuda")
+    dec, iqb = plan.empty_decoded(), plan.empty_iq()
+    dec_ms = _event_ms(lambda: plan.decode(raw, out=dec), reps, warmup)
+    dem_ms = _event_ms(lambda: plan.hilbert(dec, out=iqb), reps, warmup)
+    plan.check()
+    hbm, peak_src = measured_peaks()
+    hbm = hbm["hbm_gbs"]
+    dec_bytes, dem_bytes = T * C * 2 * S * (2 + 4), T * C * S * (2 * 4 + 8)
+    sub_c = 8
+    sub = bp.copy()
+    sub.rf_raw_dim[1] = sub_c
+    sub.dec_data_dim[1] = sub_c
+    for c in range(sub_c):
+        sub.channel_mapping[c] = c
+    raw_h = raw[:sub_c].cpu().numpy()
+    t0 = time.perf_counter()
+    O.convert_demod(raw_h, sub, taps)
+    cpu_s = time.perf_counter() - t0
+    out["bandpass"] = {
+        "workload": f"{T} tx x {C} ch x {S} complex samples (int16 IQ pairs), Hadamard, {ntaps}-tap filter",
+        "decode": {"ms": dec_ms, "achieved_gbs": dec_bytes / dec_ms / 1e6, "frac": dec_bytes / dec_ms / 1e6 / hbm,
+                   "bytes": dec_bytes},
+        "demod_filter": {"ms": dem_ms, "achieved_gbs": dem_bytes / dem_ms / 1e6,
+                         "frac": dem_bytes / dem_ms / 1e6 / hbm, "bytes": dem_bytes},
+        "peak_gbs": hbm, "peak_note": peak_src,
+        "cpu_baseline": {"ms_per_frame": cpu_s * 1e3 * C / sub_c, "cores": 1, "kind": "port",
+                         "sample": f"FP64 oracle on {sub_c} of {C} channels, scaled"}}
+    return out
+
+
 def transfer_section(reps=5):
     """The out-of-process path on the full workload: beamform_i16 from libcuda_transfer.so to a
     cutb_transfer_server process (shared-memory input and output, command socket), against the
@@ -631,6 +745,8 @@ def main():
     ap.add_argument("--precision", type=int, default=1, help="run the 256 x 256 x 8192 precision form (0: skip)")
     ap.add_argument("--motion", type=int, default=1, help="run the NCC motion-detection section (0: skip)")
     ap.add_argument("--transfer", type=int, default=1, help="run the out-of-process transfer section (0: skip)")
+    ap.add_argument("--sequences", type=int, default=1,
+                    help="run the TPW / UFORCES / bandpass section (0: skip)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
