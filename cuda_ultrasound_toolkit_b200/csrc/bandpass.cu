@@ -15,6 +15,14 @@
 // One CTA per (t, c) row: the demodulated row and the taps sit in shared memory; the phase is
 // formed as 2 pi frac(s fd / fs) from an FP64 product, so it stays exact for long rows (upstream
 // multiplies the FP32 sample index into the angle, ~1e-4 rad off at the end of a 4096-sample row).
+//
+// Filter: a thread produces kOut consecutive outputs. For outputs whose taps all fall inside the
+// row it slides a register window of 2 kOut samples through the taps, kOut taps at a time, so a
+// block of kOut taps costs kOut new samples and two 16-byte tap loads for kOut^2 complex MACs
+// (one sample and one tap load per MAC before: the loop was shared-memory bound). Each output
+// still sums its taps in ascending order with one fmaf each, so the result is unchanged; outputs
+// near the row ends take the per-output loop. Sample s sits at s + s / kOut in shared memory: the
+// lanes of a warp then read samples kOut apart without bank conflicts.
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -24,6 +32,10 @@ namespace cutb {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kOut = 8;  // consecutive outputs per thread in the filter
+
+__host__ __device__ __forceinline__ int pad_index(int s) { return s + s / kOut; }
+__host__ __device__ __forceinline__ int padded_len(int S) { return (pad_index(S) + 2) & ~1; }  // 16-byte multiple
 
 template <class OutT>
 __device__ __forceinline__ void store(OutT* out, size_t i, float2 v);
@@ -39,37 +51,90 @@ template <class OutT>
 __global__ void __launch_bounds__(kThreads) demod_fir_kernel(const float* __restrict__ in, OutT* __restrict__ out,
                                                              DemodArgs a)
 {
-    extern __shared__ float2 row[];  // S demodulated samples, then L taps (as float2.x)
-    float* taps = reinterpret_cast<float*>(row + a.S);
+    extern __shared__ float2 row[];  // S demodulated samples (padded), then the L taps reversed
+    float* trev = reinterpret_cast<float*>(row + padded_len(a.S));
     const size_t r = blockIdx.x;
     const float2* src = reinterpret_cast<const float2*>(in) + r * a.S;
-    for (int i = threadIdx.x; i < a.L; i += kThreads) taps[i] = a.taps[i];
+    for (int i = threadIdx.x; i < a.L; i += kThreads) trev[i] = a.taps[a.L - 1 - i];
     for (int s = threadIdx.x; s < a.S; s += kThreads) {
         const float2 x = __ldcs(src + s);
         const double ph = (double)s * a.fd_over_fs;
         float sn, cs;
         sincospif(2.f * (float)(ph - floor(ph)), &sn, &cs);
         // (x.x - i x.y) * (cs - i sn)
-        row[s] = make_float2(x.x * cs - x.y * sn, -x.x * sn - x.y * cs);
+        row[pad_index(s)] = make_float2(x.x * cs - x.y * sn, -x.x * sn - x.y * cs);
     }
     __syncthreads();
     OutT* dst = out + r * a.S;
     if (a.L == 0) {
-        for (int s = threadIdx.x; s < a.S; s += kThreads) store(dst, s, row[s]);
+        for (int s = threadIdx.x; s < a.S; s += kThreads) store(dst, s, row[pad_index(s)]);
         return;
     }
-    const int half = a.L / 2;
-    for (int s = threadIdx.x; s < a.S; s += kThreads) {
-        const int i0 = max(0, half - s), i1 = min(a.L, a.S + half - s);
-        float2 acc = make_float2(0.f, 0.f);
-        for (int i = i0; i < i1; ++i) {
-            const float2 z = row[s + i - half];
-            const float h = taps[a.L - 1 - i];
-            acc.x = fmaf(z.x, h, acc.x);
-            acc.y = fmaf(z.y, h, acc.y);
+    const int half = a.L / 2, L = a.L;
+    for (int s0 = threadIdx.x * kOut; s0 < a.S; s0 += kThreads * kOut) {
+        // Interior: every output s0 .. s0 + kOut - 1 exists and has all L taps inside the row
+        // (s >= half and s + L - 1 - half <= S - 1).
+        if (s0 >= half && s0 + kOut - 1 <= a.S + half - L && s0 + kOut <= a.S) {
+            const int b = s0 - half;  // sample under tap 0 of output s0
+            float2 acc[kOut], win[2 * kOut];
+#pragma unroll
+            for (int k = 0; k < kOut; ++k) acc[k] = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int j = 0; j < kOut; ++j) win[j] = row[pad_index(b + j)];
+            int i = 0;
+            for (; i + kOut <= L; i += kOut) {
+                // window: win[j] = sample b + i + j, j < 2 kOut. The top half is loaded here; this
+                // block reads win[0 .. 2 kOut - 2] (samples <= b + L + kOut - 2 <= S - 1), and
+                // win[2 kOut - 1] moves down for the next block. On the last block that sample
+                // may be index S: inside the padded shared row (padded_len(S) > pad_index(S)), unused.
+#pragma unroll
+                for (int j = kOut; j < 2 * kOut; ++j) win[j] = row[pad_index(b + i + j)];
+                float h[kOut];
+                if ((reinterpret_cast<uintptr_t>(trev + i) & 15) == 0) {
+                    const float4 h0 = *reinterpret_cast<const float4*>(trev + i);
+                    const float4 h1 = *reinterpret_cast<const float4*>(trev + i + 4);
+                    h[0] = h0.x, h[1] = h0.y, h[2] = h0.z, h[3] = h0.w;
+                    h[4] = h1.x, h[5] = h1.y, h[6] = h1.z, h[7] = h1.w;
+                } else {
+#pragma unroll
+                    for (int t = 0; t < kOut; ++t) h[t] = trev[i + t];
+                }
+#pragma unroll
+                for (int t = 0; t < kOut; ++t)
+#pragma unroll
+                    for (int k = 0; k < kOut; ++k) {
+                        acc[k].x = fmaf(win[t + k].x, h[t], acc[k].x);
+                        acc[k].y = fmaf(win[t + k].y, h[t], acc[k].y);
+                    }
+#pragma unroll
+                for (int j = 0; j < kOut; ++j) win[j] = win[j + kOut];
+            }
+            for (; i < L; ++i) {  // remaining taps (L not a multiple of kOut)
+                const float h = trev[i];
+#pragma unroll
+                for (int k = 0; k < kOut; ++k) {
+                    const float2 z = row[pad_index(b + i + k)];
+                    acc[k].x = fmaf(z.x, h, acc[k].x);
+                    acc[k].y = fmaf(z.y, h, acc[k].y);
+                }
+            }
+            const float inv = 1.f / (float)L;
+#pragma unroll
+            for (int k = 0; k < kOut; ++k) store(dst, s0 + k, make_float2(acc[k].x * inv, acc[k].y * inv));
+        } else {
+            for (int s = s0; s < min(s0 + kOut, a.S); ++s) {
+                const int i0 = max(0, half - s), i1 = min(L, a.S + half - s);
+                float2 acc = make_float2(0.f, 0.f);
+                for (int i = i0; i < i1; ++i) {
+                    const float2 z = row[pad_index(s + i - half)];
+                    const float h = trev[i];
+                    acc.x = fmaf(z.x, h, acc.x);
+                    acc.y = fmaf(z.y, h, acc.y);
+                }
+                const float inv = 1.f / (float)(i1 - i0);
+                store(dst, s, make_float2(acc.x * inv, acc.y * inv));
+            }
         }
-        const float inv = 1.f / (float)(i1 - i0);
-        store(dst, s, make_float2(acc.x * inv, acc.y * inv));
     }
 }
 
@@ -79,7 +144,7 @@ bool launch_demod_fir(const DemodArgs& a, const float* in, void* out, bool bf16,
 {
     CUTB_REQUIRE(a.rows > 0 && a.S > 0 && a.L >= 0 && (a.L == 0 || a.taps), CUTB_ERR_INVALID_ARGUMENT,
                  "Demodulation: bad arguments.");
-    const size_t smem = (size_t)a.S * sizeof(float2) + (size_t)a.L * sizeof(float);
+    const size_t smem = (size_t)padded_len(a.S) * sizeof(float2) + (size_t)a.L * sizeof(float);
     CUTB_REQUIRE(smem <= 200 * 1024, CUTB_ERR_UNSUPPORTED, "Bandpass rows of %d samples do not fit one CTA.", a.S);
     CUTB_REQUIRE(a.rows <= 0x7fffffffull, CUTB_ERR_UNSUPPORTED, "Too many rows.");
     if (bf16) {
