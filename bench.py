@@ -32,6 +32,10 @@ UNIT = "volumes/s"
 WORKLOAD = "full"
 
 
+def parallelism(world):
+    return f"frame-parallel x{world}" if world > 1 else "single GPU"
+
+
 def workload_config(extra=None):
     from cuda_ultrasound_toolkit_b200 import synth
     w = synth.CONFIGS[WORKLOAD]
@@ -130,34 +134,47 @@ def profile_traffic(name):
 
 
 # ---- CPU reference arm -------------------------------------------------------------------------------
-def cpu_sample(raw, bp, threads, frac_rows=1 / 8, frac_vox=1 / 128, seed=0):
-    """Times the FP64 oracle on a bounded sample and extrapolates seconds per volume."""
+N_VOXEL_SUBSETS = 64   # the delay-and-sum of a CPU step covers one seeded 1/64 of the voxels
+PARITY_VOXELS = 16384  # seeded voxel sample the GPU volume is compared on, against the FP64 oracle
+
+
+def voxel_subset(bp, k, n=N_VOXEL_SUBSETS, seed=0):
+    """Subset k of n disjoint, seeded voxel subsets that together cover the volume."""
+    z, y, x = bp.volume_shape
+    perm = np.random.default_rng(seed).permutation(x * y * z)
+    return np.sort(np.array_split(perm, n)[k % n])
+
+
+def cpu_sample(raw, bp, threads, subset=0, n_subsets=N_VOXEL_SUBSETS, channels=None, keep_iq=False):
+    """Times the FP64 oracle on one bounded sample of a frame and extrapolates seconds per volume:
+    convert + decode and the Hilbert analytic signal of `channels` receive channels (default: all,
+    i.e. the front end in full), and the delay-and-sum of voxel subset `subset` of `n_subsets`
+    (scaled by n_subsets). Returns (seconds per volume, description, analytic signal or None)."""
     from oracle import oracle as O
     S, C, T = bp.dims
     z, y, x = bp.volume_shape
-    sub_c = max(1, int(round(C * frac_rows)))
+    sub_c = C if channels is None else max(1, min(C, int(channels)))
     sub = bp.copy()
     sub.dec_data_dim[1] = sub_c
     t0 = time.perf_counter()
     dec = O.decode_f64(raw, sub, threads)
     t1 = time.perf_counter()
     taps = np.ctypeslib.as_array(bp.rf_filter)[: int(bp.filter_length)].astype(np.float32)
-    iq_sub = O.hilbert(dec, taps if len(taps) else None, threads)
+    iq = O.hilbert(dec, taps if len(taps) else None, threads)
     t2 = time.perf_counter()
-    # delay-and-sum needs every row: tile the sampled channels to the full aperture
-    iq = np.empty((T, C, S), np.complex128)
-    for c in range(C):
-        iq[:, c] = iq_sub[:, c % sub_c]
-    rng = np.random.default_rng(seed)
-    n_vox = max(1, int(x * y * z * frac_vox))
-    vox = rng.choice(x * y * z, n_vox, replace=False)
+    del dec
+    if sub_c < C:  # the delay-and-sum needs every row: tile the sampled channels over the aperture
+        iq = iq[:, np.arange(C) % sub_c]
+    vox = voxel_subset(bp, subset, n_subsets)
     t3 = time.perf_counter()
     O.das(iq, bp, vox, threads)
     t4 = time.perf_counter()
-    per_volume = (t1 - t0) / (sub_c / C) + (t2 - t1) / (sub_c / C) + (t4 - t3) / (n_vox / (x * y * z))
-    sample = (f"decode+Hilbert of {sub_c}/{C} receive channels, delay-and-sum of {n_vox} random voxels "
-              f"of {x * y * z}; extrapolated linearly to one volume")
-    return per_volume, sample
+    per_volume = (t2 - t0) * C / sub_c + (t4 - t3) * (x * y * z) / len(vox)
+    front = "in full" if sub_c == C else f"on {sub_c} of {C} receive channels, scaled"
+    sample = (f"FP64 oracle: convert + decode + Hilbert of {T} x {C} rows x {S} samples {front}; "
+              f"delay-and-sum of the seeded voxel subset {subset % n_subsets} of {n_subsets} ({len(vox)} of "
+              f"{x * y * z} voxels, all {T * C} rows), extrapolated linearly to one volume")
+    return per_volume, sample, (iq if keep_iq else None)
 
 
 def run_reference(args, rank):
@@ -166,22 +183,51 @@ def run_reference(args, rank):
     from cuda_ultrasound_toolkit_b200 import synth
     raw, bp = synth.frame(WORKLOAD)
     threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        cpu_sample(raw, bp, threads, frac_rows=1 / 64, frac_vox=1 / 4096)
+    for k in range(args.warmup):  # untimed: a light pass over the same code
+        cpu_sample(raw, bp, threads, subset=k, n_subsets=4096, channels=8)
     times = []
     sample = ""
     for k in range(args.steps):
-        sec, sample = cpu_sample(raw, bp, threads, frac_rows=1 / 32, frac_vox=1 / 2048, seed=k)
+        sec, sample, _ = cpu_sample(raw, bp, threads, subset=k)
         times.append(sec)
     value = len(times) / sum(times)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded phantom, 200 point scatterers, 40 dB SNR)",
-            "config": workload_config({"parallelism": "cpu threads"}),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "config": workload_config({"parallelism": parallelism(int(os.environ.get("WORLD_SIZE", "1")))}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": sample + "; step k times subset k"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def upstream_gpu_section(raw, bp, ours_vol, reps=3):
+    """Upstream's own CUDA build (baseline/_ref, built by baseline/Makefile for sm_100a) timed
+    through its cuda_toolkit::beamform on host buffers, in a child process, on the benchmark
+    frame with the settings upstream honours: cubic interpolation and no coherence factor
+    (upstream's HERCULES kernel computes the factor but never applies it). `ours_vol` is this
+    library's volume of the same frame and settings."""
+    import subprocess
+    import tempfile
+    lib = os.path.join(ROOT, "baseline", "_ref", "libcuda_toolkit_upstream.so")
+    if not os.path.exists(lib):
+        return {"unavailable": "baseline/_ref/libcuda_toolkit_upstream.so not built (make -C baseline REF=...)"}
+    with tempfile.TemporaryDirectory() as d:
+        np.save(os.path.join(d, "raw.npy"), raw)
+        with open(os.path.join(d, "params.bin"), "wb") as f:
+            f.write(bytes(bp))
+        r = subprocess.run([sys.executable, os.path.join(ROOT, "baseline", "upstream_gpu.py"), d, str(reps)],
+                           capture_output=True, text=True, timeout=600)
+        lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+        if r.returncode != 0 or not lines:
+            return {"failed": f"rc {r.returncode}: {(r.stderr or r.stdout)[-300:]}"}
+        out = json.loads(lines[-1])
+        if os.path.exists(os.path.join(d, "volume.npy")):
+            ref = np.load(os.path.join(d, "volume.npy"))
+            out["rel_l2_ours_vs_upstream"] = float(np.linalg.norm(ours_vol - ref) / np.linalg.norm(ref))
+    out["settings"] = "interpolate=true (cubic), coherency_weighting=0; same frame"
+    return out
 
 
 # ---- GPU arm ------------------------------------------------------------------------------------------------
@@ -291,7 +337,7 @@ def run_ours(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (int16 input, int32 exact decode)",
         "data": "synthetic (seeded phantom, 200 point scatterers, 40 dB SNR)",
-        "config": workload_config({"parallelism": f"frame-parallel x{world}" if world > 1 else "single GPU"}),
+        "config": workload_config({"parallelism": parallelism(world)}),
         "e2e": {"value": e2e_steps * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(raw_np[0].nbytes),
                 "d2h_bytes_per_step": int(vol_np.nbytes), "api": "cuda_toolkit::beamform (host spans)"},
         "roofline": {"bound": "fp32", "kernel": "das", "achieved": das_tflops, "peak": fp32_peak,
@@ -337,14 +383,62 @@ def run_ours(args, rank, world, local_rank):
             line["transfer"] = transfer_section()
         except Exception as exc:  # must not hide the plain pipeline's number
             line["transfer"] = {"failed": str(exc)}
+    threads = os.cpu_count() or 1
+    iq_ref = None
     try:
-        per_vol, sample = cpu_sample(frames[0][0], bp, os.cpu_count() or 1)
-        line["cpu_baseline"] = {"value": 1.0 / per_vol, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+        per_vol, sample, iq_ref = cpu_sample(frames[0][0], bp, threads, subset=0, keep_iq=True)
+        line["cpu_baseline"] = {"value": 1.0 / per_vol, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": sample}
     except Exception as exc:  # the baseline must not hide the GPU number
-        line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+        line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"failed: {exc}"}
+    try:
+        line["parity"] = full_frame_parity(plans[0], d_raw[0], frames[0][0], bp, iq_ref, threads)
+    except Exception as exc:  # must not hide the plain pipeline's number
+        line["parity"] = {"failed": str(exc)}
+    del iq_ref
+    if args.upstream and world == 1:
+        try:
+            ref_bp = bp.copy()
+            ref_bp.coherency_weighting = 0.0
+            ours = beamform(frames[0][0], ref_bp)
+            e2e_ref = []
+            for _ in range(3):
+                t = time.perf_counter()
+                beamform(frames[0][0], ref_bp, out=ours)
+                e2e_ref.append(time.perf_counter() - t)
+            up = upstream_gpu_section(frames[0][0], ref_bp, ours)
+            up["ours_same_settings"] = {"ms": 1e3 * float(np.median(e2e_ref)),
+                                        "volumes_per_s": 1.0 / float(np.median(e2e_ref)),
+                                        "api": "cuda_toolkit::beamform (host spans)"}
+            if up.get("ms"):
+                up["speedup_ours_vs_upstream"] = up["ms"] / up["ours_same_settings"]["ms"]
+            line["upstream_gpu"] = up
+        except Exception as exc:  # must not hide the plain pipeline's number
+            line["upstream_gpu"] = {"failed": str(exc)}
     print(json.dumps(line), flush=True)
+
+
+def full_frame_parity(plan, d_raw, raw, bp, iq_ref, threads):
+    """The benchmark frame's GPU result against the FP64 oracle, outside the timed region: the
+    decode bit for bit, the volume on PARITY_VOXELS seeded voxels (relative L2). iq_ref is the
+    oracle's analytic signal of the frame, when the CPU baseline has computed it."""
+    import torch
+    from oracle import oracle as O
+    dec = plan.decode(d_raw).cpu().numpy()
+    exact = bool(np.array_equal(dec, O.decode_i16(raw, bp, threads)))
+    del dec
+    vol = plan.beamform(d_raw)
+    plan.check()
+    z, y, x = bp.volume_shape
+    vox = np.sort(np.random.default_rng(21).choice(x * y * z, PARITY_VOXELS, replace=False))
+    if iq_ref is None:
+        _, _, iq_ref = cpu_sample(raw, bp, threads, keep_iq=True)
+    ref = O.das(iq_ref, bp, vox, threads)
+    got = vol.reshape(-1)[torch.from_numpy(vox).to(vol.device)].cpu().numpy()
+    return {"decode_bit_exact": exact, "rel_l2_vs_fp64": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
+            "voxels": PARITY_VOXELS, "bar": 1e-5,
+            "oracle": "FP64 decode -> Hilbert -> delay-and-sum of the same frame (oracle/oracle.cpp)"}
 
 
 def learned_path(volumes):
@@ -479,6 +573,13 @@ def precision_form(seed=3000):
     p_tc.check()
     p_bf.check()
     vol_rel = float(torch.linalg.vector_norm(vol16 - vol32) / torch.linalg.vector_norm(vol32))
+    # both volumes on a seeded voxel sample against the FP64 oracle's pipeline of the same frame
+    z, y, x = bp.volume_shape
+    vox = np.sort(rng.choice(x * y * z, 4096, replace=False))
+    ref_vox, _, _ = O.pipeline(raw.cpu().numpy(), bp, voxels=vox, threads=os.cpu_count() or 1)
+    pick = torch.from_numpy(vox).cuda()
+    v32 = vol32.reshape(-1)[pick].cpu().numpy()
+    v16 = vol16.reshape(-1)[pick].cpu().numpy()
     dec_bytes = w.T * w.C * w.S * 6
     return {"workload": "rca256 precision: 256 tx x 256 ch x 8192 samples -> 128x128x256, linear, no CF",
             "decode_tc": {"ms": tc_ms, "bit_exact_vs_fwht": exact, "achieved_gbs": dec_bytes / tc_ms / 1e6},
@@ -488,6 +589,8 @@ def precision_form(seed=3000):
                                 "sample": "64 random rows of 65536, FP64 oracle Hilbert of the same decoded rows"},
             "volume": {"das_ms_fp32_iq": das32_ms, "das_ms_bf16_iq": das16_ms,
                        "bf16_vs_fp32_iq_rel_l2": vol_rel,
+                       "fp32_iq_rel_l2_vs_fp64": rel(v32, ref_vox), "bf16_iq_rel_l2_vs_fp64": rel(v16, ref_vox),
+                       "fp64_sample": "4096 seeded voxels, FP64 oracle decode -> Hilbert -> delay-and-sum",
                        "volumes_per_s_fp32_iq": 1e3 / (tc_ms + hil32_ms + das32_ms),
                        "volumes_per_s_bf16_iq": 1e3 / (tc_ms + hil16_ms + das16_ms)}}
 
@@ -747,6 +850,8 @@ def main():
     ap.add_argument("--transfer", type=int, default=1, help="run the out-of-process transfer section (0: skip)")
     ap.add_argument("--sequences", type=int, default=1,
                     help="run the TPW / UFORCES / bandpass section (0: skip)")
+    ap.add_argument("--upstream", type=int, default=1,
+                    help="time upstream's own CUDA build on the same frame, when built in baseline/_ref (0: skip)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

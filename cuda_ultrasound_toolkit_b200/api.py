@@ -70,6 +70,7 @@ def lib():
         "cutb_debug_fail_allocations_after": ([ctypes.c_int], None),
         "cutb_calibrate_fp32": ([ctypes.POINTER(ctypes.c_double), vp], b),
         "cutb_plan_check": ([vp, vp], b),
+        "cutb_debug_das_skip_stage": ([vp, ctypes.c_int, ctypes.c_longlong], b),
         "cutb_plan_das_tile_shape": ([vp, ctypes.POINTER(u)], b),
         "cutb_batch_create": ([P, vp, u], vp),
         "cutb_batch_destroy": ([vp], None),
@@ -367,6 +368,12 @@ class Plan:
     def check(self, stream=None):
         """Synchronises the stream; raises if a device-side bounded wait gave up."""
         _check(lib().cutb_plan_check(self._h, _stream_handle(stream)), "cutb_plan_check")
+
+    def debug_skip_stage(self, stage, wait_limit_cycles=0):
+        """Test hook: the delay-and-sum never issues stage `stage` (-1: off), so its bounded wait
+        runs out after `wait_limit_cycles` (0: the default limit)."""
+        _check(lib().cutb_debug_das_skip_stage(self._h, int(stage), int(wait_limit_cycles)),
+               "cutb_debug_das_skip_stage")
 
     def beamform(self, raw, out=None, stream=None):
         out = self.empty_volume() if out is None else out

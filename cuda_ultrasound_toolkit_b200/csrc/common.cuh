@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdarg>
 #include <cstddef>
 #include <cstdint>
@@ -51,5 +52,21 @@ template <class A, class B>
 __host__ __device__ constexpr A div_up(A a, B b) { return (a + (A)b - 1) / (A)b; }
 
 inline bool is_pow2(uint64_t n) { return n && !(n & (n - 1)); }
+
+// Raises `kern`'s dynamic shared-memory limit to `bytes` on the current device. The attribute is
+// held per device, so the caller's `done` mask records the devices (bit d: device d) already set:
+// a single flag for the process would skip every device after the first. Devices past 63 set it
+// on every call. Concurrent first calls only repeat the idempotent attribute call.
+template <class Kernel>
+bool set_smem_limit(Kernel kern, size_t bytes, std::atomic<uint64_t>& done)
+{
+    int dev = 0;
+    CUTB_CUDA_OK(cudaGetDevice(&dev));
+    const uint64_t bit = dev >= 0 && dev < 64 ? 1ull << dev : 0;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return true;
+    CUTB_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    done.fetch_or(bit, std::memory_order_release);
+    return true;
+}
 
 }  // namespace cutb

@@ -7,13 +7,20 @@
 // with the constants of Beamformer::_params_to_constants (beamformer.cu:17-98) and the
 // dispatch rules of Beamformer::beamform (beamformer.cu:139-197, 223-413).
 //
-// Design. A CTA owns a tile of 4 x 8 x 32 voxels (x, y, z; FORCES: 32 x 1 x 32) and walks
-// the analytic-signal rows (t, c) in stages of 16 channels. For every row of a stage, one
-// lane of warp 0 computes the window of samples the tile can address and issues a TMA bulk
-// copy (cp.async.bulk) of exactly that window into shared memory; three stage buffers
-// with mbarrier completion keep two stages of copies in flight while all warps
-// interpolate from shared memory. Lanes of a warp are consecutive depths, whose delays
-// differ by a few samples, so the four-tap gathers do not conflict on banks.
+// Design. A CTA of four warps owns a tile of voxels: 8 x 8 x 16 (x, y, z) by default for
+// HERCULES, 4 x 8 x 32 for narrow volumes or on request, 32 x 1 x 32 for FORCES. The lanes of a
+// warp are 4 x 8 (x, y) neighbours and each thread holds 8 consecutive depths, so the lanes'
+// delays differ by a sample or two and their shared-memory reads fall in distinct banks. The CTA
+// walks the analytic-signal rows (t, c) in stages of 8 channels. The window of samples the tile
+// can address in each row follows from a Lipschitz bound on the path lengths; its metadata is
+// computed in FP64 for 8 stages at a time by all threads, and lanes 0..7 of warp 0 then copy each
+// row's window with one TMA bulk copy (cp.async.bulk) into one of three stage buffers completed
+// through an mbarrier, keeping two stages of copies in flight. Once a stage has landed, all
+// threads turn its windows into interpolation coefficients (cubic: four complex polynomial
+// coefficients per interval; linear: value and slope) in shared memory, and every voxel then
+// costs two 16-byte loads and a Horner evaluation per row, run on packed FP32x2 instructions for
+// voxel pairs. Where the windows are short enough, the coefficients are double-buffered, so a
+// stage needs one block barrier instead of two.
 //
 // Delays are formed relative to an FP64 origin at the tile centre: per row the FP64
 // distance d0 from the tile centre to the element gives the absolute sample index of the
@@ -74,13 +81,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity)
         : "memory");
     return ok != 0;
 }
-// Bounded wait: false if the phase did not complete within kWaitLimitCycles.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity)
+// Bounded wait: false if the phase did not complete within `limit` cycles.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, long long limit)
 {
     if (mbar_try_wait(bar, parity)) return true;
     const long long start = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - start > kWaitLimitCycles) return false;
+        if (clock64() - start > limit) return false;
     return true;
 }
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar)
@@ -365,6 +372,9 @@ __device__ __forceinline__ void issue_row(Smem<IQ, NC, DB>& sm, int b, int k, in
     const unsigned bytes = (unsigned)sm.next_bytes[slot][q];
     if (q == 0) sm.stage[b] = st;
     sm.row[b][q] = m;
+    // Test hook (cutb_debug_das_skip_stage): the stage is never issued, so its barrier phase never
+    // completes and the bounded wait for it gives up.
+    if (a.debug_skip && k == a.debug_skip - 1) return;
     if (bytes && m.lo + m.len - 1 == a.S) sm.raw[b][q][a.S - m.lo] = IQ{};  // zero tap past the row end
     // Order earlier generic-proxy accesses of this buffer before the async-proxy writes.
     fence_proxy_async();
@@ -384,23 +394,31 @@ __device__ __forceinline__ float path_offset(float delta, float d0, float d0sq, 
     return fmaf(-0.5f * r, res, e0);
 }
 
-// Cubic coefficients of every staged interval of stage buffer b (all threads).
+// Interpolation coefficients of every staged interval of stage buffer b (all threads). The
+// (row, interval) pairs are dealt out over the whole CTA: a staged row has at most `wint`
+// intervals (i = 1 .. len - 3), and item e is interval 1 + e mod wint of row e / wint, so every
+// thread builds about nq * wint / kThreads of them. A per-row loop over i left the threads past
+// the window length idle (a 60-sample window keeps two of four warps busy) while the others
+// built, and the idle warps then waited at the stage barrier.
 template <class IQ, int NC, bool DB>
-__device__ __forceinline__ void build_coefficients(Smem<IQ, NC, DB>& sm, int b, int nq, int cb)
+__device__ __forceinline__ void build_coefficients(Smem<IQ, NC, DB>& sm, int b, int nq, int cb, int wint,
+                                                   float rwint)
 {
     if (threadIdx.x < nq) sm.rowc[cb][threadIdx.x] = sm.row[b][threadIdx.x];
-    for (int q = 0; q < nq; ++q) {
-        const int len = sm.row[b][q].len;
+    const int n = nq * wint;
+#pragma unroll 1
+    for (int e = threadIdx.x; e < n; e += kThreads) {
+        // e / wint: (e + 1/2) / wint is at least 1 / (2 wint) from an integer, far above the
+        // rounding of the product (e < 2^11).
+        const int q = (int)(((float)e + 0.5f) * rwint);
+        const int i = 1 + e - q * wint;
+        if (i > sm.row[b][q].len - 3) continue;
         const IQ* p = &sm.raw[b][q][0];
         if constexpr (NC == 1) {
             // linear: value(t) = p0 + t (p1 - p0), the operations of the scalar staged pass
-            for (int i = 1 + threadIdx.x; i <= len - 3; i += kThreads) {
-                const float2 p0 = to_f2(p[i]), p1 = to_f2(p[i + 1]);
-                sm.coefA[cb][q][i] = make_float4(p0.x, p0.y, p1.x - p0.x, p1.y - p0.y);
-            }
-            continue;
+            const float2 p0 = to_f2(p[i]), p1 = to_f2(p[i + 1]);
+            sm.coefA[cb][q][i] = make_float4(p0.x, p0.y, p1.x - p0.x, p1.y - p0.y);
         } else {
-        for (int i = 1 + threadIdx.x; i <= len - 3; i += kThreads) {
             const float2 pm1 = to_f2(p[i - 1]), p0 = to_f2(p[i]), p1 = to_f2(p[i + 1]), p2 = to_f2(p[i + 2]);
             float4 A, B;
             A.x = p0.x;
@@ -413,7 +431,6 @@ __device__ __forceinline__ void build_coefficients(Smem<IQ, NC, DB>& sm, int b, 
             B.w = fmaf(0.5f, p2.y - pm1.y, 1.5f * (p0.y - p1.y));
             sm.coefA[cb][q][i] = A;
             sm.coefB[cb][q][i] = B;
-        }
         }
     }
 }
@@ -677,6 +694,14 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
     __syncthreads();
     tile.tx_reach = HERC ? __int_as_float(sm.tx_reach_bits) : tile.radius * a.spm;
 
+    // Intervals per staged row, at most: compute_row's window spans i_lo - 2 - (SA - 1) ..
+    // i_hi + 3 with i_hi - i_lo <= floor(2 reach) + 1 (reach is uniform over the tile), so
+    // len - 3 <= floor(2 reach) + 3 + SA; a staged row also has len <= kWin - SA.
+    constexpr int SA = 16 / sizeof(IQ);
+    const int wint = min((int)floor(2.0 * ((double)tile.radius * (double)a.spm + (double)tile.tx_reach + 1.0)) + 3 + SA,
+                         Smem<IQ, NC, DB>::kWin - 3);
+    const float rwint = __frcp_rn((float)wint);
+
     // |delta|^2 and the z part of -2 (e - centre).delta, per voxel.
     const float two_cz = (float)(2.0 * tile.cz);
     float qz[kVpt];
@@ -714,10 +739,12 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
     if (warp == 0 && lane < kRows)
         for (int j = 0; j < kStages && k_begin + j < nstages; ++j) issue_row(sm, j, k_begin + j, lane, a, iq);
 
+    const long long wait_limit = a.wait_limit > 0 ? a.wait_limit : kWaitLimitCycles;
+    int j_abort = -1;  // local stage at which the loop gave up
     for (int k = k_begin; k < nstages; ++k) {
         const int j = k - k_begin;  // local stage number: buffer and barrier phase
         const int b = j % kStages;
-        if (!mbar_wait_bounded(&sm.full[b], (unsigned)(j / kStages) & 1u)) {
+        if (!mbar_wait_bounded(&sm.full[b], (unsigned)(j / kStages) & 1u, wait_limit)) {
             sm.abort[j & 1] = 1;
             atomicOr(a.status, 1);
         }
@@ -733,9 +760,12 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
         // (j + 1) % kStages, metadata ring slots of stages j + kStages + 1 onwards.
         const int cb = DB ? (j & 1) : 0;
         if constexpr (NC > 0) {
-            build_coefficients(sm, b, st.nq, cb);
+            build_coefficients(sm, b, st.nq, cb, wint, rwint);
             all_staged = __syncthreads_and(threadIdx.x >= st.nq || sm.row[b][threadIdx.x].len > 0);
-            if (DB && sm.abort[j & 1]) break;
+            if (DB && sm.abort[j & 1]) {
+                j_abort = j;
+                break;
+            }
             // The raw buffer is free once transformed: refill it while this stage computes.
             if (warp == 0 && lane < kRows && next < nstages && !sm.abort[j & 1]) issue_row(sm, b, next, lane, a, iq);
         }
@@ -806,13 +836,19 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
         }
         if constexpr (!DB) {
             __syncthreads();
-            if (sm.abort[j & 1]) break;
+            if (sm.abort[j & 1]) {
+                j_abort = j;
+                break;
+            }
         }
         if (NC == 0 && warp == 0 && lane < kRows && next < nstages) issue_row(sm, b, next, lane, a, iq);
     }
-    if (sm.abort[0] | sm.abort[1]) {
-        // Let every copy already issued land before the CTA's shared memory is released.
-        for (int k = 0; k < kStages; ++k) mbar_wait_bounded(&sm.full[k], 0), mbar_wait_bounded(&sm.full[k], 1);
+    if (j_abort >= 0) {
+        // Stages j_abort + 1 .. j_abort + kStages - 1 were issued before the loop gave up (the
+        // refill of stage j_abort's buffer was not); let their copies land before the CTA's shared
+        // memory is released. Stage j_abort itself is the one whose wait ran out.
+        for (int m = j_abort + 1; m < j_abort + kStages && k_begin + m < nstages; ++m)
+            mbar_wait_bounded(&sm.full[m % kStages], (unsigned)(m / kStages) & 1u, wait_limit);
         return;
     }
 
@@ -911,11 +947,8 @@ bool launch_das_k(const DasArgs& a, const void* iq, void* volume, cudaStream_t s
     CUTB_REQUIRE(grid.y <= 65535 && grid.z <= 65535, CUTB_ERR_UNSUPPORTED, "Output grid too large.");
     auto kern = das_kernel<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>;
     const size_t smem = sizeof(Smem<IQ, coef_arrays<SEQ, CUBIC, APO>(), DB>);
-    static bool configured = false;
-    if (!configured) {
-        CUTB_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured = true;
-    }
+    static std::atomic<uint64_t> smem_set{0};
+    if (!set_smem_limit(kern, smem, smem_set)) return false;
     kern<<<grid, kThreads, smem, st>>>((const IQ*)iq, (float2*)volume, a);
     CUTB_CUDA_OK(cudaGetLastError());
     return true;

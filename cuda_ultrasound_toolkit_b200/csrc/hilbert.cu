@@ -18,6 +18,7 @@
 // radix-16 pass once, at the start (all three transforms share them), and forms the pass's
 // 15 twiddles as products of those: a per-butterfly table read per twiddle had kept the
 // load/store unit saturated (0.73 ms -> 0.31 ms on 16384 rows of 4096 samples).
+#include <atomic>
 #include <cmath>
 #include <complex>
 #include <vector>
@@ -66,8 +67,23 @@ template <int LOGN>
 constexpr int hilbert_threads() { return hilbert_fft_per_block<LOGN>() * (1 << LOGN) / 16; }
 template <int LOGN>
 constexpr int hilbert_min_blocks() { return hilbert_threads<LOGN>() <= 256 ? 2 : 1; }
+// At 2^14 points the pair form needs 256 KiB of shared memory (exchange buffers + the held
+// product), above the 227 KiB a CTA may have; one row per CTA needs only the exchange buffers.
+template <int LOGN>
+constexpr bool hilbert_single_row() { return LOGN >= 14; }
+template <int LOGN>
+constexpr size_t hilbert_smem_bytes()
+{
+    constexpr size_t N = size_t(1) << LOGN;
+    return hilbert_fft_per_block<LOGN>() *
+           (2 * fft::spad_size(N) * sizeof(float) + (hilbert_single_row<LOGN>() ? 0 : N * sizeof(float2)));
+}
+static_assert(hilbert_smem_bytes<14>() <= 227 * 1024 && hilbert_smem_bytes<13>() <= 227 * 1024, "shared memory");
 
-template <int LOGN, class OutT>
+// PAD: rows of a.n samples (any length) transformed at the power-of-two length N >= 2 a.n - 1 with
+// zeros appended; the spectral tables then hold the weight of the equivalent length-N circular
+// convolution (build_hilbert_tables), and only the first a.n outputs are stored.
+template <int LOGN, class OutT, bool PAD>
 __global__ void __launch_bounds__(hilbert_threads<LOGN>(), hilbert_min_blocks<LOGN>())
 hilbert_kernel(const float* __restrict__ in, OutT* __restrict__ out, HilbertArgs a)
 {
@@ -75,12 +91,14 @@ hilbert_kernel(const float* __restrict__ in, OutT* __restrict__ out, HilbertArgs
     constexpr uint32_t TPF = N / 16;
     constexpr uint32_t FPB = hilbert_fft_per_block<LOGN>();
     constexpr uint32_t PN = fft::spad_size(N);
+    constexpr bool SINGLE = hilbert_single_row<LOGN>();
     extern __shared__ float smem[];
 
+    const uint32_t L = PAD ? a.n : N;  // samples per row in memory
     const uint32_t grp = threadIdx.x / TPF, tau = threadIdx.x % TPF;
     const uint64_t pair = (uint64_t)blockIdx.x * FPB + grp;
-    const uint64_t ra = 2 * pair, rb = ra + 1;
-    const bool has_a = ra < a.rows, has_b = rb < a.rows;
+    const uint64_t ra = SINGLE ? (uint64_t)blockIdx.x : 2 * pair, rb = ra + 1;
+    const bool has_a = ra < a.rows, has_b = !SINGLE && rb < a.rows;
     float* sre = smem + grp * 2 * PN;
     float* sim = sre + PN;
     const cplx* tw = reinterpret_cast<const cplx*>(a.twiddle);
@@ -91,8 +109,9 @@ hilbert_kernel(const float* __restrict__ in, OutT* __restrict__ out, HilbertArgs
 #pragma unroll
     for (int m = 0; m < 16; ++m) {
         const uint64_t n = tau + m * TPF;
-        z[m].x = has_a ? __ldcs(in + (ra * N + n) * a.in_stride) : 0.f;
-        z[m].y = has_b ? __ldcs(in + (rb * N + n) * a.in_stride) : 0.f;
+        const bool in_row = !PAD || n < L;
+        z[m].x = has_a && in_row ? __ldcs(in + (ra * L + n) * a.in_stride) : 0.f;
+        z[m].y = has_b && in_row ? __ldcs(in + (rb * L + n) * a.in_stride) : 0.f;
     }
     run_fft<LOGN, -1>(z, tau, tw, sre, sim, wb);  // z[m] = Z[tau + m*TPF]
 
@@ -102,6 +121,22 @@ hilbert_kernel(const float* __restrict__ in, OutT* __restrict__ out, HilbertArgs
         const float2 v = __ldg(t + k);
         return cplx{v.x, v.y};
     };
+    if constexpr (SINGLE) {
+        // One real row: iq = IDFT(X G) with G = Ge + i Go.
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const uint32_t k = tau + m * TPF;
+            const cplx e = weight(ge, k), o = weight(go, k);
+            z[m] = fft::cmul(z[m], cplx{e.x - o.y, e.y + o.x});
+        }
+        run_fft<LOGN, +1>(z, tau, tw, sre, sim, wb);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const uint64_t n = tau + m * TPF;
+            if (has_a && (!PAD || n < L)) store_iq(out, ra * L + n, z[m].x, z[m].y);
+        }
+        return;
+    } else {
     // IDFT(Z Ge) = Re(iq_a) + i Re(iq_b) and IDFT(Z Go) = Im(iq_a) + i Im(iq_b). Z Go waits in this
     // thread's own slots of `keep` while the first inverse transform runs, then the first result
     // waits there during the second, and every output sample is written once, whole. Only one
@@ -126,89 +161,153 @@ hilbert_kernel(const float* __restrict__ in, OutT* __restrict__ out, HilbertArgs
 #pragma unroll
     for (int m = 0; m < 16; ++m) {
         const uint64_t n = tau + m * TPF;
+        if (PAD && n >= L) continue;
         const float2 r = keep[n];
-        if (has_a) store_iq(out, ra * N + n, r.x, z[m].x);
-        if (has_b) store_iq(out, rb * N + n, r.y, z[m].y);
+        if (has_a) store_iq(out, ra * L + n, r.x, z[m].x);
+        if (has_b) store_iq(out, rb * L + n, r.y, z[m].y);
+    }
     }
 }
 
-template <int LOGN, class OutT>
+template <int LOGN, class OutT, bool PAD>
 bool launch_hilbert_t(const float* in, void* out, const HilbertArgs& a, cudaStream_t st)
 {
-    constexpr uint32_t N = 1u << LOGN;
     constexpr uint32_t FPB = hilbert_fft_per_block<LOGN>();
-    const size_t smem = (size_t)FPB * (2 * fft::spad_size(N) * sizeof(float) + N * sizeof(float2));
-    auto kern = hilbert_kernel<LOGN, OutT>;
-    static bool configured = false;
-    if (!configured) {
-        CUTB_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured = true;
-    }
-    const uint64_t pairs = (a.rows + 1) / 2;
-    const uint64_t blocks = div_up(pairs, (uint64_t)FPB);
+    constexpr size_t smem = hilbert_smem_bytes<LOGN>();
+    auto kern = hilbert_kernel<LOGN, OutT, PAD>;
+    static std::atomic<uint64_t> smem_set{0};
+    if (!set_smem_limit(kern, smem, smem_set)) return false;
+    const uint64_t units = hilbert_single_row<LOGN>() ? a.rows : (a.rows + 1) / 2;  // rows or row pairs
+    const uint64_t blocks = div_up(units, (uint64_t)FPB);
     CUTB_REQUIRE(blocks <= 0x7fffffffull, CUTB_ERR_INVALID_ARGUMENT, "Too many rows for one launch.");
     kern<<<(unsigned)blocks, hilbert_threads<LOGN>(), smem, st>>>(in, (OutT*)out, a);
     CUTB_CUDA_OK(cudaGetLastError());
     return true;
 }
 
-template <class OutT>
+template <class OutT, bool PAD>
 bool launch_hilbert_o(const float* in, void* out, const HilbertArgs& a, cudaStream_t st)
 {
     switch (a.log_n) {
-        case 4: return launch_hilbert_t<4, OutT>(in, out, a, st);
-        case 5: return launch_hilbert_t<5, OutT>(in, out, a, st);
-        case 6: return launch_hilbert_t<6, OutT>(in, out, a, st);
-        case 7: return launch_hilbert_t<7, OutT>(in, out, a, st);
-        case 8: return launch_hilbert_t<8, OutT>(in, out, a, st);
-        case 9: return launch_hilbert_t<9, OutT>(in, out, a, st);
-        case 10: return launch_hilbert_t<10, OutT>(in, out, a, st);
-        case 11: return launch_hilbert_t<11, OutT>(in, out, a, st);
-        case 12: return launch_hilbert_t<12, OutT>(in, out, a, st);
-        case 13: return launch_hilbert_t<13, OutT>(in, out, a, st);
-        case 14: return launch_hilbert_t<14, OutT>(in, out, a, st);
+        case 4: return launch_hilbert_t<4, OutT, PAD>(in, out, a, st);
+        case 5: return launch_hilbert_t<5, OutT, PAD>(in, out, a, st);
+        case 6: return launch_hilbert_t<6, OutT, PAD>(in, out, a, st);
+        case 7: return launch_hilbert_t<7, OutT, PAD>(in, out, a, st);
+        case 8: return launch_hilbert_t<8, OutT, PAD>(in, out, a, st);
+        case 9: return launch_hilbert_t<9, OutT, PAD>(in, out, a, st);
+        case 10: return launch_hilbert_t<10, OutT, PAD>(in, out, a, st);
+        case 11: return launch_hilbert_t<11, OutT, PAD>(in, out, a, st);
+        case 12: return launch_hilbert_t<12, OutT, PAD>(in, out, a, st);
+        case 13: return launch_hilbert_t<13, OutT, PAD>(in, out, a, st);
+        case 14: return launch_hilbert_t<14, OutT, PAD>(in, out, a, st);
         default: break;
     }
     set_error(CUTB_ERR_UNSUPPORTED, "Hilbert transform length 2^%u not supported.", a.log_n);
     return false;
 }
 
+using cd = std::complex<double>;
+
+// In-place FP64 radix-2 FFT (power-of-two length), sum_j a[j] exp(sign 2 pi i j k / n); the
+// twiddles come from exact index arithmetic.
+void fft_fp64(std::vector<cd>& a, int sign)
+{
+    const size_t n = a.size();
+    for (size_t i = 1, j = 0; i < n; ++i) {
+        size_t bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) std::swap(a[i], a[j]);
+    }
+    const double two_pi = 6.283185307179586476925286766559;
+    std::vector<cd> w(n / 2);
+    for (size_t k = 0; k < n / 2; ++k) w[k] = std::polar(1.0, sign * two_pi * (double)k / (double)n);
+    for (size_t len = 2; len <= n; len <<= 1) {
+        const size_t half = len / 2, step = n / len;
+        for (size_t i = 0; i < n; i += len)
+            for (size_t k = 0; k < half; ++k) {
+                const cd u = a[i + k], v = a[i + k + half] * w[k * step];
+                a[i + k] = u + v;
+                a[i + k + half] = u - v;
+            }
+    }
+}
+
 }  // namespace
 
-bool hilbert_supported_length(unsigned n) { return is_pow2(n) && n >= 16 && n <= kMaxHilbertLength; }
+unsigned hilbert_fft_length(unsigned n)
+{
+    if (n == 0) return 0;
+    if (is_pow2(n) && n >= 16) return n <= kMaxHilbertLength ? n : 0;
+    unsigned m = 16;
+    while (m < 2 * (uint64_t)n - 1) m <<= 1;
+    return m <= kMaxHilbertLength ? m : 0;
+}
 
-// Host tables: twiddles exp(-2*pi*i*m/N) and the Hermitian parts of the spectral weight
-// G = w * F, all computed in double and rounded once to float.
+bool hilbert_supported_length(unsigned n) { return hilbert_fft_length(n) != 0; }
+
+// Host tables, all computed in double and rounded once to float: twiddles exp(-2*pi*i*m/M) of the
+// FFT length M = hilbert_fft_length(n) and the Hermitian parts of the spectral weight.
+//
+// Power-of-two rows (M = n): the weight is G = w * F itself.
+//
+// Other lengths: upstream's cuFFT transforms at the row length n itself. The filter-and-mask step
+// is a length-n circular convolution, iq[j] = sum_m x[m] g[(j - m) mod n], with the kernel
+// g[j] = sum_k G[k] exp(+2 pi i k j / n) = (taps circularly convolved with mk)[j], where
+// mk[j] = sum_{k <= n/2} w_k exp(2 pi i k j / n) has the closed form
+//   mk[0] = (0.75 + 1.5 K) / n,  mk[j] = (0.75 + 1.5 e^{i pi j (K+1)/n} sin(pi j K / n) / sin(pi j / n)) / n
+// (K = floor(n/2), a geometric series). The same convolution of the zero-padded row follows from a
+// length-M circular convolution with h, h[j] = g[j] and h[M - j] = g[n - j] (the negative lags),
+// which do not overlap when M >= 2n - 1; its spectral weight is DFT_M(h) / M (the kernel's inverse
+// transform is unnormalised). Only outputs 0..n-1 are kept.
 bool build_hilbert_tables(unsigned n, const float* taps, unsigned ntaps, std::vector<float>& twiddle,
                           std::vector<float>& ge, std::vector<float>& go)
 {
-    CUTB_REQUIRE(hilbert_supported_length(n), CUTB_ERR_UNSUPPORTED,
-                 "Sample count %u not supported by the FFT (powers of two 16..%u).", n, kMaxHilbertLength);
+    const unsigned M = hilbert_fft_length(n);
+    CUTB_REQUIRE(M != 0, CUTB_ERR_UNSUPPORTED,
+                 "Sample count %u not supported by the FFT (powers of two up to %u, other lengths up to %u).", n,
+                 kMaxHilbertLength, kMaxHilbertLength / 2);
     CUTB_REQUIRE(ntaps <= n, CUTB_ERR_INVALID_ARGUMENT, "Match filter longer (%u) than the sample count (%u).", ntaps,
                  n);
-    using cd = std::complex<double>;
-    const double two_pi = 6.283185307179586476925286766559;
-    twiddle.resize(2 * (size_t)n);
-    std::vector<cd> root(n);
-    for (unsigned m = 0; m < n; ++m) {
-        root[m] = std::polar(1.0, -two_pi * (double)m / (double)n);
+    const double two_pi = 6.283185307179586476925286766559, pi = two_pi / 2;
+    twiddle.resize(2 * (size_t)M);
+    std::vector<cd> root(M);
+    for (unsigned m = 0; m < M; ++m) {
+        root[m] = std::polar(1.0, -two_pi * (double)m / (double)M);
         twiddle[2 * m] = (float)root[m].real();
         twiddle[2 * m + 1] = (float)root[m].imag();
     }
-    std::vector<cd> g(n, cd(0, 0));
-    const unsigned half = n / 2;
-    for (unsigned k = 0; k <= half; ++k) {
-        cd f(1.0, 0.0);
-        if (ntaps) {
-            f = 0;
-            for (unsigned t = 0; t < ntaps; ++t) f += (double)taps[t] * root[(uint64_t)k * t % n];
+    std::vector<cd> g(M, cd(0, 0));
+    if (M == n) {
+        const unsigned half = n / 2;
+        for (unsigned k = 0; k <= half; ++k) {
+            cd f(1.0, 0.0);
+            if (ntaps) {
+                f = 0;
+                for (unsigned t = 0; t < ntaps; ++t) f += (double)taps[t] * root[(uint64_t)k * t % n];
+            }
+            g[k] = ((k == 0 ? 0.75 : 1.5) / (double)n) * f;
         }
-        g[k] = ((k == 0 ? 0.75 : 1.5) / (double)n) * f;
+    } else {
+        const uint64_t K = n / 2, two_n = 2 * (uint64_t)n;
+        std::vector<cd> mk(n), gt(n, cd(0, 0));
+        mk[0] = (0.75 + 1.5 * (double)K) / (double)n;
+        for (uint64_t j = 1; j < n; ++j) {
+            const double ratio = std::sin(pi * (double)(j * K % two_n) / n) / std::sin(pi * (double)j / n);
+            mk[j] = (0.75 + 1.5 * std::polar(ratio, pi * (double)(j * (K + 1) % two_n) / n)) / (double)n;
+        }
+        if (ntaps == 0) gt = mk;
+        for (unsigned t = 0; t < ntaps; ++t)
+            for (unsigned j = 0; j < n; ++j) gt[j] += (double)taps[t] * mk[(j + n - t) % n];
+        for (unsigned j = 0; j < n; ++j) g[j] = gt[j];
+        for (unsigned j = 1; j < n; ++j) g[M - j] = gt[n - j];
+        fft_fp64(g, -1);
+        for (auto& v : g) v /= (double)M;
     }
-    ge.resize(2 * (size_t)n);
-    go.resize(2 * (size_t)n);
-    for (unsigned k = 0; k < n; ++k) {
-        const cd gm = std::conj(g[(n - k) % n]);
+    ge.resize(2 * (size_t)M);
+    go.resize(2 * (size_t)M);
+    for (unsigned k = 0; k < M; ++k) {
+        const cd gm = std::conj(g[(M - k) % M]);
         const cd e = 0.5 * (g[k] + gm);
         const cd o = (g[k] - gm) / cd(0.0, 2.0);
         ge[2 * k] = (float)e.real();
@@ -221,7 +320,12 @@ bool build_hilbert_tables(unsigned n, const float* taps, unsigned ntaps, std::ve
 
 bool launch_hilbert(const HilbertArgs& a, const float* in, void* out, bool bf16, cudaStream_t st)
 {
-    return bf16 ? launch_hilbert_o<__nv_bfloat162>(in, out, a, st) : launch_hilbert_o<float2>(in, out, a, st);
+    CUTB_REQUIRE(a.n >= 1 && hilbert_fft_length(a.n) == (1u << a.log_n), CUTB_ERR_INVALID_ARGUMENT,
+                 "Hilbert rows of %u samples do not match the transform length 2^%u.", a.n, a.log_n);
+    const bool pad = a.n != (1u << a.log_n);
+    if (pad) return bf16 ? launch_hilbert_o<__nv_bfloat162, true>(in, out, a, st)
+                         : launch_hilbert_o<float2, true>(in, out, a, st);
+    return bf16 ? launch_hilbert_o<__nv_bfloat162, false>(in, out, a, st) : launch_hilbert_o<float2, false>(in, out, a, st);
 }
 
 }  // namespace cutb

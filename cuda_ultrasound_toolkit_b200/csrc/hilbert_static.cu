@@ -9,8 +9,10 @@
 // This entry point keeps those tables in a fixed file-scope device array instead, so every
 // byte it touches is either the caller's input/output or that array.
 //
-// The array holds the tables of one transform of up to kStaticMaxSamples samples per row
-// (384 KiB); every GPU that loads the library keeps it until the process exits. Each call
+// The array holds the tables of one transform of up to kStaticMaxSamples points (384 KiB): rows
+// of up to 16384 samples when the count is a power of two, up to 8192 otherwise (those run as a
+// zero-padded transform of at least twice the length). Every GPU that loads the library keeps the
+// array until the process exits. Each call
 // rewrites all the tables it needs, on the caller's stream, before the kernel reads them, so
 // nothing in the array has to start at zero. All calls share the array: calls that overlap
 // on the GPU (on different streams, or issued from several host threads) race on it and must
@@ -25,6 +27,7 @@ namespace cutb {
 namespace {
 
 constexpr unsigned kStaticMaxSamples = 16384;
+static_assert(kStaticMaxSamples >= kMaxHilbertLength, "the array must hold the longest transform's tables");
 constexpr int kMaxDevices = 64;
 
 // twiddle | Ge | Go, kStaticMaxSamples complex values each.
@@ -66,21 +69,23 @@ extern "C" CUTB_API bool cutb_hilbert_static(const float* d_in, uint in_stride, 
                  "cutb_hilbert_static: %u samples per row exceed the fixed table capacity of %u.", samples,
                  kStaticMaxSamples);
     CUTB_REQUIRE(hilbert_supported_length(samples), CUTB_ERR_UNSUPPORTED,
-                 "Sample count %u not supported by the FFT (powers of two 16..%u).", samples, kMaxHilbertLength);
+                 "Sample count %u not supported by the FFT (powers of two up to %u, other lengths up to %u).",
+                 samples, kMaxHilbertLength, kMaxHilbertLength / 2);
     CUTB_REQUIRE(ntaps == 0 || taps, CUTB_ERR_INVALID_ARGUMENT, "Null match filter.");
     std::vector<float> tw, ge, go;  // host memory only
     if (!build_hilbert_tables(samples, taps, ntaps, tw, ge, go)) return false;
     float* tables = nullptr;
     if (!table_address(&tables)) return false;
     cudaStream_t st = (cudaStream_t)stream;
-    const size_t n = 2 * (size_t)samples;
+    const size_t n = tw.size();  // 2 floats per point of the FFT length (<= kStaticMaxSamples)
     CUTB_CUDA_OK(cudaMemcpyAsync(tables, tw.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
     CUTB_CUDA_OK(cudaMemcpyAsync(tables + n, ge.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
     CUTB_CUDA_OK(cudaMemcpyAsync(tables + 2 * n, go.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
     HilbertArgs a{};
     a.rows = rows;
+    a.n = samples;
     a.log_n = 0;
-    while ((1u << a.log_n) < samples) ++a.log_n;
+    while ((1u << a.log_n) < n / 2) ++a.log_n;
     a.in_stride = in_stride;
     a.twiddle = tables;
     a.ge = tables + n;

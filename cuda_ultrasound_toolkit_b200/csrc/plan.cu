@@ -175,8 +175,9 @@ bool FrontEnd::set_filter(const float* taps, uint32_t ntaps)
     CUTB_CUDA_OK(
         cudaMemcpy(d_tables + 2 * tw.size(), go.data(), go.size() * sizeof(float), cudaMemcpyHostToDevice));
     hil.rows = (uint64_t)T * C;
+    hil.n = S;
     hil.log_n = 0;
-    while ((1u << hil.log_n) < S) ++hil.log_n;
+    while ((1u << hil.log_n) < tw.size() / 2) ++hil.log_n;
     hil.twiddle = d_tables;
     hil.ge = d_tables + tw.size();
     hil.go = d_tables + 2 * tw.size();
@@ -249,7 +250,8 @@ bool FrontEnd::hilbert(const float* d_in, unsigned in_stride, void* d_iq, bool b
         return launch_demod_fir(demod_args, d_in, d_iq, bf16, st);
     }
     CUTB_REQUIRE(fft_ok && d_tables != nullptr, CUTB_ERR_UNSUPPORTED,
-                 "Sample count %u not supported by the FFT (powers of two 16..%u).", S, kMaxHilbertLength);
+                 "Sample count %u not supported by the FFT (powers of two up to %u, other lengths up to %u).", S,
+                 kMaxHilbertLength, kMaxHilbertLength / 2);
     CUTB_REQUIRE(in_stride == 1 || in_stride == 2, CUTB_ERR_INVALID_ARGUMENT, "Input stride must be 1 or 2.");
     CUTB_REQUIRE(d_in && d_iq, CUTB_ERR_INVALID_ARGUMENT, "Null device buffer.");
     HilbertArgs a = hil;
@@ -395,6 +397,18 @@ CUTB_API bool cutb_plan_check(cutb_plan* p, void* stream)
         set_error(CUTB_ERR_TIMEOUT, "A device-side wait of the delay-and-sum kernel gave up (status %#x).", status);
         return false;
     }
+    return true;
+}
+
+CUTB_API bool cutb_debug_das_skip_stage(cutb_plan* p, int stage, long long wait_limit_cycles)
+{
+    CUTB_REQUIRE(p, CUTB_ERR_INVALID_ARGUMENT, "Null plan.");
+    CUTB_REQUIRE(stage >= -1 && wait_limit_cycles >= 0, CUTB_ERR_INVALID_ARGUMENT,
+                 "Stage must be -1 (off) or a stage index, the wait limit non-negative.");
+    CUTB_REQUIRE(p->das.seq == HERCULES || p->das.seq == FORCES, CUTB_ERR_UNSUPPORTED,
+                 "Only the staged (HERCULES / FORCES) delay-and-sum has bounded waits.");
+    p->das.debug_skip = stage + 1;
+    p->das.wait_limit = wait_limit_cycles;
     return true;
 }
 

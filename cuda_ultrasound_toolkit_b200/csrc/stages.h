@@ -57,14 +57,18 @@ bool launch_demod_fir(const DemodArgs& a, const float* in, void* out, bool bf16,
 constexpr unsigned kMaxHilbertLength = 16384;
 
 struct HilbertArgs {
-    uint64_t rows;             // T * C rows of N samples
-    uint32_t log_n;            // N = 2^log_n
+    uint64_t rows;             // T * C rows of n samples
+    uint32_t n;                // samples per row
+    uint32_t log_n;            // FFT length 2^log_n = hilbert_fft_length(n): n, or >= 2 n - 1 for other lengths
     uint32_t in_stride;        // 1: packed floats, 2: real part of complex input
-    const float* twiddle;      // device: N complex exp(-2 pi i m / N)
-    const float* ge;           // device: N complex, Hermitian-even part of the spectral weight
-    const float* go;           // device: N complex, Hermitian-odd part (divided by i)
+    const float* twiddle;      // device: 2^log_n complex exp(-2 pi i m / 2^log_n)
+    const float* ge;           // device: 2^log_n complex, Hermitian-even part of the spectral weight
+    const float* go;           // device: 2^log_n complex, Hermitian-odd part (divided by i)
 };
 
+// FFT length for rows of n samples: n itself for powers of two from 16, else the power of two
+// >= max(16, 2 n - 1) (zero-padded circular convolution); 0 when above kMaxHilbertLength.
+unsigned hilbert_fft_length(unsigned n);
 bool hilbert_supported_length(unsigned n);
 bool build_hilbert_tables(unsigned n, const float* taps, unsigned ntaps, std::vector<float>& twiddle,
                           std::vector<float>& ge, std::vector<float>& go);
@@ -101,6 +105,8 @@ struct DasArgs {
     int ntiles;
     int splits;                // > 1: stages split across CTAs, partial sums added atomically
     int* status;               // device word: bit 0 set when a bounded wait gave up
+    long long wait_limit;      // cycles a bounded wait spins before giving up (0: about 0.2 s)
+    int debug_skip;            // test hook: stage debug_skip - 1 is never issued (0: off)
 };
 
 // One frame of a persistent batched delay-and-sum: its constants and device buffers.

@@ -30,7 +30,9 @@ namespace cuda_toolkit
                             std::span<uint8_t> output_data,
                             const CudaBeamformerParameters& bp);
 
-    /* Outside the RF -> volume path: log and return false so the link surface matches. */
+    /* NCC block-matching motion detection over host frames (upstream cuda_toolkit.cpp:202):
+     * images holds frame_count float32 frames, motion_maps receives a float4 per grid point and
+     * frame (dx, dy, peak, no-shift peak). Returns false and logs on error. */
     EXPORT_FN bool motion_detection(std::span<const uint8_t> images,
                                     std::span<uint8_t> motion_maps,
                                     const NccMotionParameters& params);

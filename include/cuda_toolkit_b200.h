@@ -87,7 +87,9 @@ CUTB_API bool cutb_decode(cutb_plan* plan, const void* d_raw, size_t raw_bytes, 
 
 /* Match-filtered analytic signal of every [T][C] row: d_in f32 with element stride in_stride
  * (1 = packed, 2 = real part of complex) -> d_iq complex [T][C][S] (complex64, or bf16x2
- * when the plan stores bf16). */
+ * when the plan stores bf16). S: any power of two up to 16384, any other count up to 8192
+ * (computed as a zero-padded circular convolution of the same result); longer rows report
+ * CUTB_ERR_UNSUPPORTED. */
 CUTB_API bool cutb_hilbert(cutb_plan* plan, const float* d_in, uint in_stride, void* d_iq, void* stream);
 
 /* Delay-and-sum of d_iq [T][C][S] into the complex64 volume d_volume [Z][Y][X]. */
@@ -135,6 +137,14 @@ CUTB_API int cutb_batch_das_launches(const cutb_batch* batch);
  * wait (CUTB_ERR_TIMEOUT); clears the flag. cuda_toolkit::beamform calls it on every frame. */
 CUTB_API bool cutb_plan_check(cutb_plan* plan, void* stream);
 
+/* Test hook for the bounded waits of the staged delay-and-sum (HERCULES / FORCES): from the next
+ * call on, stage `stage` (transmit x channel-group step, counted from 0 in every CTA) is never
+ * issued, so the wait for its copies runs out after wait_limit_cycles (0: the default of about
+ * 0.2 s), the CTA stops, waits for the copies it had already issued and leaves; cutb_plan_check
+ * then reports CUTB_ERR_TIMEOUT. stage = -1 turns the hook off. The volume of such a call is
+ * undefined. No GPU fault is involved: every wait stays bounded. */
+CUTB_API bool cutb_debug_das_skip_stage(cutb_plan* plan, int stage, long long wait_limit_cycles);
+
 /* Number of kernels the last cutb_beamform/cutb_decode/cutb_hilbert/cutb_das call launched. */
 CUTB_API int cutb_plan_last_launch_count(const cutb_plan* plan);
 
@@ -145,8 +155,10 @@ CUTB_API int cutb_plan_last_launch_count(const cutb_plan* plan);
  * host has reserved the memory. No plan and no allocation: d_in holds rows x samples floats with
  * element stride in_stride (1 or 2), d_iq receives rows x samples complex64, taps/ntaps is the
  * match filter in host memory (ntaps <= samples, 0 = none). The FFT tables live in a fixed device
- * array sized for samples <= 16384 (384 KiB, held by every GPU that loads the library until the
- * process exits); longer rows are rejected with CUTB_ERR_INVALID_ARGUMENT. The first call on a
+ * array sized for transforms of up to 16384 points (384 KiB, held by every GPU that loads the
+ * library until the process exits): rows of up to 16384 samples when the count is a power of two,
+ * up to 8192 otherwise. Rows longer than 16384 are rejected with CUTB_ERR_INVALID_ARGUMENT, other
+ * unsupported counts with CUTB_ERR_UNSUPPORTED. The first call on a
  * device looks up that array's address, so make it before any stream capture. Every call rewrites
  * the array on `stream`; calls that overlap on the GPU race on it and must be serialised. */
 CUTB_API bool cutb_hilbert_static(const float* d_in, uint in_stride, void* d_iq, uint samples, size_t rows,

@@ -250,13 +250,17 @@ void dft(std::vector<cd>& a, int sign)
         j ^= bit;
         if (i < j) std::swap(a[i], a[j]);
     }
+    /* w[k] = exp(sign 2 pi i k / n); stage `len` uses w[k * n / len] (the same angles, from one table) */
+    std::vector<cd> w(n / 2);
+    for (size_t k = 0; k < n / 2; ++k) {
+        double ang = sign * 2.0 * M_PI * (double)k / (double)n;
+        w[k] = cd(std::cos(ang), std::sin(ang));
+    }
     for (size_t len = 2; len <= n; len <<= 1) {
-        size_t half = len / 2;
+        size_t half = len / 2, step = n / len;
         for (size_t i = 0; i < n; i += len)
             for (size_t k = 0; k < half; ++k) {
-                double ang = sign * 2.0 * M_PI * (double)k / (double)len;
-                cd w(std::cos(ang), std::sin(ang));
-                cd u = a[i + k], v = a[i + k + half] * w;
+                cd u = a[i + k], v = a[i + k + half] * w[k * step];
                 a[i + k] = u + v;
                 a[i + k + half] = u - v;
             }

@@ -38,6 +38,11 @@ FRONTEND = [
     ("t8_c4_s256_pad_filter", 8, 4, 256, 13, 3, 32, 2),
     ("t12_c4_s64_base12", 12, 4, 64, 0, 0, 16, 3),
     ("t20_c3_s64_base20", 20, 3, 64, 5, 1, 0, 4),
+    # sample counts that are not powers of two (upstream's cuFFT plans any length)
+    ("t4_c3_s100_filter", 4, 3, 100, 0, 0, 16, 5),
+    ("t8_c2_s2500_pad_filter", 8, 2, 2500, 3, 1, 64, 6),
+    ("t12_c2_s3072", 12, 2, 3072, 0, 0, 0, 7),
+    ("t4_c2_s6000_filter", 4, 2, 6000, 0, 0, 64, 8),
 ]
 
 # Delay-and-sum cases on one small frame (T=8, C=8, S=512, volume 12 x 6 x 20). Upstream always

@@ -36,7 +36,7 @@ def test_encoding_matrices_match_upstream(orc, native):
 def test_frontend_matches_upstream(orc):
     g = _load("frontend.npz")
     names = sorted(k[:-4] for k in g.files if k.endswith(".raw"))
-    assert len(names) == 4
+    assert len(names) == 8  # 4 power-of-two and 4 other sample counts
     for n in names:
         bp = _params(g[n + ".params"])
         dec = orc.decode_i16(g[n + ".raw"], bp)

@@ -103,7 +103,10 @@ def test_decode_f32_general(torch, orc):
 # ---------------------------------------------------------------------------------------------
 # Hilbert
 # ---------------------------------------------------------------------------------------------
-@pytest.mark.parametrize("N", [16, 64, 256, 1024, 2048, 4096, 8192])
+# Powers of two run at their own length (16384: one row per CTA); other counts as a zero-padded
+# transform of at least twice the length (8191: the longest, padded to 16384).
+@pytest.mark.parametrize("N", [16, 64, 256, 1024, 2048, 4096, 8192, 16384,
+                               8, 100, 127, 1001, 2500, 3072, 6000, 8191])
 @pytest.mark.parametrize("taps", [0, 64])
 def test_hilbert_vs_fp64(torch, orc, N, taps):
     T, C = 3, 5                                    # 15 rows: odd count exercises the unpaired row
@@ -385,6 +388,21 @@ def test_pipeline_small_vs_oracle(torch, orc, small_frame):
     assert rel_l2(vol.ravel()[vox], ref) < TOL_VOLUME
 
 
+@pytest.mark.parametrize("S", [1000, 2500])
+def test_pipeline_sample_count_not_power_of_two(torch, orc, S):
+    """Whole pipeline with rows whose length is not a power of two (the analytic signal runs as a
+    zero-padded transform), against the FP64 oracle's decode -> Hilbert (length-S DFT) -> DAS."""
+    w = synth.Workload("np2", 8, 8, S, 16, 8, 32, 4, cubic=True, cf=1.0, filter_taps=16, z_range=(5e-3, 15e-3),
+                       box_xy=2e-3)
+    raw, cmap, _, _ = synth.synth_frame(w, 9)
+    bp = synth.make_params(w, channel_map=cmap)
+    plan = Plan(bp)
+    vol = plan.beamform(torch.from_numpy(raw).cuda()).cpu().numpy()
+    plan.check()
+    ref, _, _ = orc.pipeline(raw, bp)
+    assert rel_l2(vol, ref) < 1e-4
+
+
 def test_host_span_entry_points(torch, small_frame):
     raw, bp = small_frame
     ref = Plan(bp).beamform(torch.from_numpy(raw).cuda()).cpu().numpy()
@@ -445,9 +463,10 @@ def test_invalid_parameters_are_rejected(torch):
         with pytest.raises(CutbError) as e:
             Plan(bp)
         assert e.value.code == code, e.value
-    plan = Plan(base_params(100, C, T))              # decode works, the FFT length does not
+    # decode works, the FFT length does not (not a power of two, and over 8192)
+    plan = Plan(base_params(8196, C, T))
     with pytest.raises(CutbError) as e:
-        plan.beamform(torch.zeros(100 * T * C, dtype=torch.int16, device="cuda"))
+        plan.beamform(torch.zeros(8196 * T * C, dtype=torch.int16, device="cuda"))
     assert e.value.code == 2
 
 
