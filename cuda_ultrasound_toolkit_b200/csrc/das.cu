@@ -205,6 +205,7 @@ struct alignas(128) Smem {
     // other slot, so all threads leave the stage loop at the same stage.
     int abort[2];
     int tx_reach_bits;
+    int part_last;  // stream-K: the pair counter's value before this part's arrival
 };
 
 // Coefficient arrays staged per row: cubic always 2; linear 1 where the packed row pass runs
@@ -400,14 +401,18 @@ __device__ __forceinline__ float path_offset(float delta, float d0, float d0sq, 
 // thread builds about nq * wint / kThreads of them. A per-row loop over i left the threads past
 // the window length idle (a 60-sample window keeps two of four warps busy) while the others
 // built, and the idle warps then waited at the stage barrier.
+//
+// Threads first .. first + count - 1 share the items (all threads, or the ones that are not
+// computing window metadata in this stage).
 template <class IQ, int NC, bool DB>
 __device__ __forceinline__ void build_coefficients(Smem<IQ, NC, DB>& sm, int b, int nq, int cb, int wint,
-                                                   float rwint)
+                                                   float rwint, int first, int count)
 {
     if (threadIdx.x < nq) sm.rowc[cb][threadIdx.x] = sm.row[b][threadIdx.x];
     const int n = nq * wint;
+    if ((int)threadIdx.x < first) return;
 #pragma unroll 1
-    for (int e = threadIdx.x; e < n; e += kThreads) {
+    for (int e = (int)threadIdx.x - first; e < n; e += count) {
         // e / wint: (e + 1/2) / wint is at least 1 / (2 wint) from an integer, far above the
         // rounding of the product (e < 2^11).
         const int q = (int)(((float)e + 0.5f) * rwint);
@@ -625,12 +630,21 @@ struct Layout {
     static constexpr int TZ = (kShort ? 2 : kWarps) * kVpt;
 };
 
-// One tile (bx, by, bz) of the volume, stage slice `split` of a.splits. Called by the grid
+// Parts of a tile under the stream-K decomposition (das_stream_kernel): the whole stage range, or
+// the first or the last part of a tile whose stages two consecutive CTAs share.
+constexpr int kPartFull = 0, kPartHead = 1, kPartTail = 2;
+constexpr int kTileVoxels = kThreads * kVpt;
+static_assert(kTileVoxels == (int)kStreamTileVoxels, "stream-K scratch holds one record per voxel of a tile");
+
+// Stages of one tile: transmits x channel groups x READI sub-signals.
+__host__ __device__ __forceinline__ int tile_stages(const DasArgs& a) { return a.T * div_up(a.C, kRows) * a.G; }
+
+// One tile (bx, by, bz) of the volume, stages k_lo .. k_hi - 1. Called by the grid
 // kernel (a in parameter space) and by the persistent batch kernel (a in its parameter table).
 template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT, bool DB = false>
 __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __restrict__ vol, const DasArgs& a,
                                          Smem<IQ, coef_arrays<SEQ, CUBIC, APO>(), DB>& sm, int bx, int by, int bz,
-                                         int split)
+                                         int k_lo, int k_hi, int part = kPartFull, int pair = 0)
 {
     constexpr int NC = coef_arrays<SEQ, CUBIC, APO>();
     static_assert(!DB || NC > 0, "two coefficient buffers need coefficients");
@@ -727,10 +741,7 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
     }
 
     const int nchunks = div_up(a.C, kRows);
-    const int total_stages = a.T * nchunks * a.G;
-    // This CTA's stages: all of them, or slice `split` of a.splits.
-    const int k_begin = a.splits > 1 ? (int)((long long)total_stages * split / a.splits) : 0;
-    const int nstages = a.splits > 1 ? (int)((long long)total_stages * (split + 1) / a.splits) : total_stages;
+    const int k_begin = k_lo, nstages = k_hi;
     // Window metadata (FP64) is computed for kBatch stages at a time by all threads; a stage's
     // bulk copies are then issued by lanes 0..kRows-1 of warp 0, one row per lane.
     static_assert(kRows <= 32 && kStages <= kBatch, "issue layout");
@@ -750,8 +761,13 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
         }
         const StageMeta st = sm.stage[b];
         const int next = k + kStages;  // stage that refills buffer b
-        if (next < nstages && (next - k_begin) % kBatch == 0)
-            compute_batch<SEQ>(sm, next, nstages, nchunks, a, tile);
+        // Every kBatch stages the first kBatch * kRows threads compute the next batch of window
+        // metadata, one row each, and the other threads build this stage's coefficients alone,
+        // so that both halves of the CTA reach the stage barrier together.
+        constexpr int kMeta = kBatch * kRows;
+        static_assert(kMeta < kThreads, "metadata rows leave threads for the coefficients");
+        const bool batch = next < nstages && (next - k_begin) % kBatch == 0;
+        if (batch) compute_batch<SEQ>(sm, next, nstages, nchunks, a, tile);
         int all_staged = 1;
         // DB: stage j builds into coefficient buffer j % 2, last read by stage j - 2's rows, which
         // every warp finished before the barrier below in stage j - 1; so the end-of-stage
@@ -760,7 +776,8 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
         // (j + 1) % kStages, metadata ring slots of stages j + kStages + 1 onwards.
         const int cb = DB ? (j & 1) : 0;
         if constexpr (NC > 0) {
-            build_coefficients(sm, b, st.nq, cb, wint, rwint);
+            if (batch) build_coefficients(sm, b, st.nq, cb, wint, rwint, kMeta, kThreads - kMeta);
+            else build_coefficients(sm, b, st.nq, cb, wint, rwint, 0, kThreads);
             all_staged = __syncthreads_and(threadIdx.x >= st.nq || sm.row[b][threadIdx.x].len > 0);
             if (DB && sm.abort[j & 1]) {
                 j_abort = j;
@@ -863,6 +880,30 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
             inc[v] += ix + iy;
         }
     }
+    if (part != kPartFull) {
+        // Stream-K: two consecutive CTAs summed the two parts of this tile's stages. Each writes its
+        // sums to its own slot of the pair's scratch, then counts its arrival; the second to arrive
+        // adds the other part's sums and finishes the tile. Addition of the two parts commutes, so
+        // the result does not depend on which part arrives last. Nothing waits for the other part.
+        float4* mine = a.sk_partials + ((size_t)pair * 2 + (part == kPartTail ? 1 : 0)) * kTileVoxels;
+        const float4* other = a.sk_partials + ((size_t)pair * 2 + (part == kPartTail ? 0 : 1)) * kTileVoxels;
+#pragma unroll
+        for (int v = 0; v < kVpt; ++v) mine[threadIdx.x * kVpt + v] = make_float4(total[v].x, total[v].y, inc[v], 0.f);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) sm.part_last = atomicAdd(a.sk_counters + pair, 1);
+        __syncthreads();
+        if (sm.part_last == 0) return;  // the other part finishes the tile
+        __threadfence();
+#pragma unroll
+        for (int v = 0; v < kVpt; ++v) {
+            const float4 o = __ldcg(other + threadIdx.x * kVpt + v);
+            total[v].x += o.x;
+            total[v].y += o.y;
+            inc[v] += o.z;
+        }
+        if (threadIdx.x == 0) a.sk_counters[pair] = 0;  // ready for the next launch
+    }
     if (x_idx >= a.X || y_idx >= a.Y) return;
 #pragma unroll
     for (int v = 0; v < kVpt; ++v) {
@@ -897,16 +938,55 @@ das_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
     auto& sm = *reinterpret_cast<Smem<IQ, coef_arrays<SEQ, CUBIC, APO>(), DB>*>(smem_raw);
     using L = Layout<SEQ, SHORT>;
     int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
-    int split = 0;
+    const int nst = tile_stages(a);
+    int k_lo = 0, k_hi = nst;
     if (a.tiles) {
         const int nx = div_up(a.X, L::TX), ny = div_up(a.Y, L::TY);
         const int id = a.tiles[blockIdx.x];
         bx = id % nx;
         by = (id / nx) % ny;
         bz = id / (nx * ny);
-        split = blockIdx.y;
+        if (a.splits > 1) {  // this CTA's slice blockIdx.y of a.splits
+            k_lo = (int)((long long)nst * blockIdx.y / a.splits);
+            k_hi = (int)((long long)nst * (blockIdx.y + 1) / a.splits);
+        }
     }
-    das_tile<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>(iq, vol, a, sm, bx, by, bz, split);
+    das_tile<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>(iq, vol, a, sm, bx, by, bz, k_lo, k_hi);
+}
+
+// Stream-K form of the grid kernel for volumes of more than one wave of tiles: gridDim.x CTAs
+// (one wave: SMs x resident CTAs) split the whole work, tiles x stages, into equal contiguous
+// ranges, so that the last wave is not left partly empty. A CTA walks the tiles of its range in
+// id order (z-major, then y, then x); a tile cut by a range boundary is finished by the second of
+// its two CTAs (the part protocol of das_tile, through a.sk_partials / a.sk_counters). Each range
+// spans at least one tile (gridDim.x <= tiles), so a tile has at most two parts, and the first part
+// of a tile that CTA c cuts lies in c, the last in c + 1: pair c.
+template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT, bool DB>
+__global__ void __launch_bounds__(kThreads, 3)
+das_stream_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    auto& sm = *reinterpret_cast<Smem<IQ, coef_arrays<SEQ, CUBIC, APO>(), DB>*>(smem_raw);
+    using L = Layout<SEQ, SHORT>;
+    const int nx = div_up(a.X, L::TX), ny = SEQ == HERCULES ? div_up(a.Y, L::TY) : 1;
+    const long long nst = tile_stages(a);
+    const long long work = (long long)nx * ny * div_up(a.Z, L::TZ) * nst;
+    const long long s1 = work * (blockIdx.x + 1) / gridDim.x;
+    long long s = work * blockIdx.x / gridDim.x;
+    while (s < s1) {
+        const long long tile = s / nst;
+        const int k0 = (int)(s - tile * nst), k1 = (int)min(nst, s1 - tile * nst);
+        const int part = k0 > 0 ? kPartTail : (k1 < nst ? kPartHead : kPartFull);
+        const int pair = part == kPartTail ? (int)blockIdx.x - 1 : (int)blockIdx.x;
+        das_tile<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>(iq, vol, a, sm, (int)(tile % nx), (int)((tile / nx) % ny),
+                                                     (int)(tile / ((long long)nx * ny)), k0, k1, part, pair);
+        s = tile * nst + k1;
+        __syncthreads();
+        if (sm.abort[0] | sm.abort[1]) break;
+        if (threadIdx.x == 0)
+            for (int b = 0; b < kStages; ++b) mbar_inval(&sm.full[b]);
+        __syncthreads();
+    }
 }
 
 // Persistent delay-and-sum over the tiles of many frames: CTAs take (frame, tile) work items,
@@ -929,7 +1009,7 @@ das_batch_kernel(const DasBatchParams P, const int2* __restrict__ items, int nit
         const DasFrame& f = P.f[w.x];
         const int nx = div_up(f.a.X, L::TX), ny = div_up(f.a.Y, L::TY);
         das_tile<SEQ, CUBIC, CF, APO, IQ, SHORT>((const IQ*)f.iq, f.vol, f.a, sm, w.y % nx, (w.y / nx) % ny,
-                                                 w.y / (nx * ny), 0);
+                                                 w.y / (nx * ny), 0, tile_stages(f.a));
         __syncthreads();
         if (sm.abort[0] | sm.abort[1]) break;
         if (threadIdx.x == 0)
@@ -938,17 +1018,56 @@ das_batch_kernel(const DasBatchParams P, const int2* __restrict__ items, int nit
     }
 }
 
+// CTAs of `kern` that one wave holds on the current device (SMs x resident CTAs), cached per
+// device in `cache` (0: not yet known).
+template <class Kernel>
+bool wave_size(Kernel kern, size_t smem, std::atomic<int> (&cache)[64], int* wave)
+{
+    int dev = 0;
+    CUTB_CUDA_OK(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && (*wave = cache[dev].load(std::memory_order_relaxed)) > 0) return true;
+    int sms = 0, per_sm = 0;
+    CUTB_CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CUTB_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem));
+    *wave = sms * per_sm;
+    if (dev >= 0 && dev < 64) cache[dev].store(*wave, std::memory_order_relaxed);
+    return true;
+}
+
+// Set by prepare_das: launch_das_k only sets the kernel attributes and caches the wave size.
+thread_local bool g_prepare_only = false;
+
 template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT, bool DB>
 bool launch_das_k(const DasArgs& a, const void* iq, void* volume, cudaStream_t st)
 {
     using L = Layout<SEQ, SHORT>;
-    dim3 grid(div_up(a.X, L::TX), div_up(a.Y, L::TY), div_up(a.Z, L::TZ));
+    // FORCES does not depend on y: one y-slice of tiles, each written to every y.
+    dim3 grid(div_up(a.X, L::TX), SEQ == HERCULES ? div_up(a.Y, L::TY) : 1, div_up(a.Z, L::TZ));
     if (a.tiles) grid = dim3(a.ntiles, a.splits > 1 ? a.splits : 1, 1);
     CUTB_REQUIRE(grid.y <= 65535 && grid.z <= 65535, CUTB_ERR_UNSUPPORTED, "Output grid too large.");
     auto kern = das_kernel<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>;
     const size_t smem = sizeof(Smem<IQ, coef_arrays<SEQ, CUBIC, APO>(), DB>);
+    if (!a.tiles && a.sk_partials && a.sk_counters) {
+        // More than one wave of tiles that is not a whole number of waves: the stream-K form
+        // spreads the last, partly empty wave's work over every CTA.
+        auto skern = das_stream_kernel<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>;
+        static std::atomic<uint64_t> sk_smem_set{0};
+        static std::atomic<int> sk_wave[64];
+        if (!set_smem_limit(skern, smem, sk_smem_set)) return false;
+        int wave = 0;
+        if (!wave_size(skern, smem, sk_wave, &wave)) return false;
+        const long long tiles = (long long)grid.x * grid.y * grid.z;
+        if (g_prepare_only) return true;
+        if (wave > 1 && tiles > wave && tiles % wave != 0 && wave - 1 <= a.sk_capacity) {
+            CUTB_CUDA_OK(cudaMemsetAsync(a.sk_counters, 0, sizeof(int) * (size_t)wave, st));
+            skern<<<wave, kThreads, smem, st>>>((const IQ*)iq, (float2*)volume, a);
+            CUTB_CUDA_OK(cudaGetLastError());
+            return true;
+        }
+    }
     static std::atomic<uint64_t> smem_set{0};
     if (!set_smem_limit(kern, smem, smem_set)) return false;
+    if (g_prepare_only) return true;
     kern<<<grid, kThreads, smem, st>>>((const IQ*)iq, (float2*)volume, a);
     CUTB_CUDA_OK(cudaGetLastError());
     return true;
@@ -1197,6 +1316,7 @@ void das_grid_tiles(const DasArgs& a, int counts[3])
     int shape[3];
     das_tile_shape(a, shape);
     for (int i = 0; i < 3; ++i) counts[i] = div_up(i == 0 ? a.X : i == 1 ? a.Y : a.Z, shape[i]);
+    if (a.seq != HERCULES) counts[1] = 1;  // y-invariant: one slice of tiles
 }
 
 void das_tile_shape(const DasArgs& a, int shape[3])
@@ -1205,6 +1325,15 @@ void das_tile_shape(const DasArgs& a, int shape[3])
     shape[0] = a.seq == HERCULES ? (sh ? Layout<HERCULES, true>::TX : Layout<HERCULES, false>::TX) : Layout<FORCES, false>::TX;
     shape[1] = a.seq == HERCULES ? 8 : 1;
     shape[2] = sh ? Layout<HERCULES, true>::TZ : Layout<HERCULES, false>::TZ;
+}
+
+bool prepare_das(const DasArgs& a, bool iq_bf16)
+{
+    if (a.seq != HERCULES && a.seq != FORCES) return true;
+    g_prepare_only = true;
+    const bool ok = launch_das(a, nullptr, iq_bf16, nullptr, nullptr, nullptr);
+    g_prepare_only = false;
+    return ok;
 }
 
 bool launch_das(const DasArgs& a, const void* iq, bool iq_bf16, void* volume, cudaStream_t st, int* launches)

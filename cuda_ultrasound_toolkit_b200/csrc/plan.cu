@@ -484,6 +484,24 @@ bool cutb_plan::build(const CudaBeamformerParameters& params, const cutb_options
     CUTB_CUDA_OK(cudaMemset(d_status, 0, sizeof(int)));
     das.status = d_status;
     if (opt.decode_tc && !fe.enable_tc_decode(d_status)) return false;
+    if (das.seq == HERCULES || das.seq == FORCES) {
+        // Stream-K scratch of the staged delay-and-sum, for volumes of more than one wave of tiles.
+        int dev = 0, sms = 0, counts[3];
+        CUTB_CUDA_OK(cudaGetDevice(&dev));
+        CUTB_CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        das_grid_tiles(das, counts);
+        if ((long long)counts[0] * counts[1] * counts[2] > sms) {
+            const int pairs = sms * kStreamPairsPerSm;
+            if (!alloc_bytes((void**)&d_sk_partials, sizeof(float4) * 2 * kStreamTileVoxels * (size_t)pairs))
+                return false;
+            if (!alloc_bytes((void**)&d_sk_counters, sizeof(int) * (size_t)pairs)) return false;
+            CUTB_CUDA_OK(cudaMemset(d_sk_counters, 0, sizeof(int) * (size_t)pairs));
+            das.sk_partials = d_sk_partials;
+            das.sk_counters = d_sk_counters;
+            das.sk_capacity = pairs;
+        }
+        if (!prepare_das(das, iq_bf16)) return false;
+    }
     return true;
 }
 
@@ -504,4 +522,6 @@ cutb_plan::~cutb_plan()
     device_free(d_tiles);
     device_free(d_angles);
     device_free(d_elems);
+    device_free(d_sk_partials);
+    device_free(d_sk_counters);
 }

@@ -56,6 +56,8 @@ struct cutb_plan {
     int* d_tiles = nullptr;    // tile list of cutb_das_tiles
     float* d_angles = nullptr; // RCA_TPW plane-wave angles
     short* d_elems = nullptr;  // UFORCES transmit elements
+    float4* d_sk_partials = nullptr;  // stream-K partial sums of the delay-and-sum (large volumes)
+    int* d_sk_counters = nullptr;
     uint32_t tiles_capacity = 0;
     int launches = 0;
 

@@ -105,6 +105,9 @@ struct DasArgs {
     int ntiles;
     int splits;                // > 1: stages split across CTAs, partial sums added atomically
     int* status;               // device word: bit 0 set when a bounded wait gave up
+    float4* sk_partials;       // stream-K scratch: 2 x kTileVoxels partial sums per pair of CTAs (null: off)
+    int* sk_counters;          // stream-K: arrivals per pair of CTAs, zeroed before each launch
+    int sk_capacity;           // pairs the scratch holds
     long long wait_limit;      // cycles a bounded wait spins before giving up (0: about 0.2 s)
     int debug_skip;            // test hook: stage debug_skip - 1 is never issued (0: off)
 };
@@ -136,6 +139,12 @@ void das_grid_tiles(const DasArgs& a, int counts[3]);
 // validation as the upstream dispatcher (beamformer.cu:17-197).
 bool derive_das(const CudaBeamformerParameters& bp, DasArgs& a);
 bool launch_das(const DasArgs& a, const void* iq, bool iq_bf16, void* volume, cudaStream_t st, int* launches);
+// Sets the shared-memory attributes of the kernels `a` will launch on the current device and
+// caches their wave sizes, without launching (call outside stream capture, e.g. at plan creation).
+bool prepare_das(const DasArgs& a, bool iq_bf16);
+// Stream-K scratch for a device with `sms` SMs: pairs and bytes of the partial sums.
+constexpr int kStreamPairsPerSm = 4;
+constexpr size_t kStreamTileVoxels = 1024;
 // Tilted-plane-wave and UFORCES delay-and-sum (das_direct.cu).
 bool launch_das_direct(const DasArgs& a, const void* iq, bool iq_bf16, void* volume, cudaStream_t st);
 // Tile shape (x, y, z voxels) the delay-and-sum kernel uses for these arguments.

@@ -16,11 +16,15 @@ Phantoms: 50-400 point scatterers with U(0.5, 1) amplitudes plus 20 000 speckle 
 with N(0, 0.05) amplitudes, uniform in the box; phantom k is seeded by k.
 
 NRMSE = ||V_hat - V|| / ||V|| over the complex volume, V the plain full-transmit volume.
-Gate: the full-transmit front end runs, and the full-transmit delay-and-sum is evaluated on a
-fixed, seeded 1/64 of the delay-and-sum tiles (cutb_das_tiles, stages split over CTAs); its
-NRMSE against the restored volume on those voxels is the estimate. Above 2 % the volume falls
-back to the full-transmit delay-and-sum of the already decoded analytic signal, whose cost is
-charged to the learned path.
+Gate: the full-transmit front end runs, and the full-transmit delay-and-sum is evaluated on 1/64
+of the delay-and-sum tiles (cutb_das_tiles, stages split over CTAs). The tiles are drawn with
+probability proportional to half the restored volume's energy in the tile plus half a uniform
+share (systematic PPS sampling; tiles whose share would exceed one draw are always taken), and
+the squared NRMSE is estimated as the ratio of the Horvitz-Thompson estimates of sum |V_hat - V|^2
+and sum |V|^2 over those tiles. Uniformly drawn tiles mostly missed the few bright tiles that
+hold most of the energy, and their estimate was off by ~0.04 at NRMSE ~0.4. Above 2 % the volume
+falls back to the full-transmit delay-and-sum of the already decoded analytic signal, whose cost
+is charged to the learned path.
 
   python -m cuda_ultrasound_toolkit_b200.sparse train --phantoms 2048 --epochs 4 --out weights.npz
   python -m cuda_ultrasound_toolkit_b200.sparse evaluate --weights weights.npz --phantoms 256
@@ -173,16 +177,7 @@ class LearnedPath:
         self.vg = torch.empty_like(self.vf)
         self.dec = self.full.plan.empty_decoded()
         self.iq = self.full.plan.empty_iq()
-        tx, ty, tz = self.full.plan.tile_shape
-        nx, ny, nz = -(-X // tx), -(-Y // ty), -(-Z // tz)
-        n = nx * ny * nz
-        rng = np.random.default_rng(20260101)
-        self.gate_tiles = np.sort(rng.choice(n, max(1, n // GATE_FRACTION), replace=False)).astype(np.int32)
-        mask = torch.zeros((Z, Y, X), dtype=torch.bool)
-        for i in self.gate_tiles:
-            x, y, z = i % nx, (i // nx) % ny, i // (nx * ny)
-            mask[z * tz:(z + 1) * tz, y * ty:(y + 1) * ty, x * tx:(x + 1) * tx] = True
-        self.mask = mask.cuda()
+        self.gate = Gate(self.full.plan.tile_shape, GRID)
 
     def run(self, scat, seed):
         """Acquires both schemes (untimed), then times the learned path's stages and the plain
@@ -199,10 +194,10 @@ class LearnedPath:
         plan.decode(self.full.raw, out=self.dec)
         plan.hilbert(self.dec, out=self.iq)
         ev[3].record()
-        plan.das_tiles(self.iq, self.gate_tiles, splits=GATE_SPLITS, out=self.vg)
+        tiles, weights = self.gate.choose(self.vo[0], seed)
+        plan.das_tiles(self.iq, tiles, splits=GATE_SPLITS, out=self.vg)
         self.vg /= self.full.gain
-        g = self.vg[self.mask]
-        est = torch.linalg.vector_norm(self.vo[0][self.mask] - g) / torch.linalg.vector_norm(g)
+        est = self.gate.estimate(self.vo[0], self.vg, tiles, weights)
         ev[4].record()
         plan.das(self.iq, out=self.vf)   # plain path's delay-and-sum, also the fallback
         self.vf /= self.full.gain
@@ -211,6 +206,70 @@ class LearnedPath:
         t = [ev[i].elapsed_time(ev[i + 1]) for i in range(5)]
         return dict(sparse_ms=t[0], unet_ms=t[1], front_ms=t[2], gate_ms=t[3], das_ms=t[4], gate_nrmse=float(est),
                     nrmse_net=nrmse(self.vo[0], self.vf), nrmse_plain=nrmse(self.vs[0], self.vf))
+
+
+class Gate:
+    """Spot check of a restored volume against the full-transmit delay-and-sum on 1 in
+    GATE_FRACTION tiles. choose() picks the tiles from the restored volume (one device-to-host
+    copy of its 2048 tile energies), estimate() returns the NRMSE estimate from the restored
+    volume and the full-transmit delay-and-sum of the chosen tiles."""
+
+    def __init__(self, tile_shape, grid, fraction=GATE_FRACTION, uniform_share=0.5):
+        self.tx, self.ty, self.tz = tile_shape
+        Z, Y, X = grid
+        self.nx, self.ny, self.nz = -(-X // self.tx), -(-Y // self.ty), -(-Z // self.tz)
+        assert (self.nx * self.tx, self.ny * self.ty, self.nz * self.tz) == (X, Y, Z), "whole tiles only"
+        self.ntiles = self.nx * self.ny * self.nz
+        self.n = max(1, self.ntiles // fraction)
+        self.uniform_share = uniform_share
+
+    def tile_sums(self, v):
+        """Sum over each tile of v (Z, Y, X) -> tile id order (z-major, then y, then x)."""
+        t = v.reshape(self.nz, self.tz, self.ny, self.ty, self.nx, self.tx)
+        return t.sum(dim=(1, 3, 5)).reshape(-1)
+
+    def choose(self, restored, seed):
+        """(tile ids int32, Horvitz-Thompson weights 1 / inclusion probability) for this volume."""
+        energy = self.tile_sums(restored.real.square() + restored.imag.square()).double().cpu().numpy()
+        N, n = self.ntiles, self.n
+        tot = energy.sum()
+        p = (1 - self.uniform_share) * (energy / tot if tot > 0 else np.full(N, 1.0 / N)) + self.uniform_share / N
+        certain = np.zeros(N, dtype=bool)
+        while True:  # tiles that would be drawn with probability >= 1 are taken outright
+            rest = np.flatnonzero(~certain)
+            m = n - int(certain.sum())
+            q = p[rest] / p[rest].sum()
+            big = rest[q * m >= 1.0]
+            if len(big) == 0 or m <= 0:
+                break
+            certain[big] = True
+        rest = np.flatnonzero(~certain)
+        m = n - int(certain.sum())
+        tiles, weights = list(np.flatnonzero(certain)), [1.0] * int(certain.sum())
+        if m > 0:
+            q = p[rest] / p[rest].sum()
+            start = np.random.default_rng(seed).random()
+            picks = np.searchsorted(np.cumsum(q), (start + np.arange(m)) / m, side="right")
+            picks = np.minimum(picks, len(rest) - 1)
+            tiles += list(rest[picks])
+            weights += list(1.0 / (m * q[picks]))
+        # a tile drawn twice (only possible through rounding at the edge q m -> 1) is listed once,
+        # with its weights added: the delay-and-sum adds the partial sums of a listed tile
+        ids, inv = np.unique(np.asarray(tiles, dtype=np.int64), return_inverse=True)
+        w = np.zeros(len(ids))
+        np.add.at(w, inv, np.asarray(weights, dtype=np.float64))
+        return ids.astype(np.int32), w
+
+    def estimate(self, restored, full_tiles, tiles, weights):
+        """NRMSE estimate: sqrt(HT(sum |restored - full|^2) / HT(sum |full|^2)) over the tiles."""
+        d = restored - full_tiles
+        err = self.tile_sums(d.real.square() + d.imag.square())
+        en = self.tile_sums(full_tiles.real.square() + full_tiles.imag.square())
+        idx = torch.from_numpy(tiles.astype(np.int64)).to(restored.device)
+        w = torch.from_numpy(weights).to(restored.device)
+        num = (err.index_select(0, idx).double() * w).sum()
+        den = (en.index_select(0, idx).double() * w).sum()
+        return float(torch.sqrt(num / den))
 
 
 def summarize(rows, bar=NRMSE_BAR):

@@ -92,7 +92,10 @@ CUTB_API bool cutb_decode(cutb_plan* plan, const void* d_raw, size_t raw_bytes, 
  * CUTB_ERR_UNSUPPORTED. */
 CUTB_API bool cutb_hilbert(cutb_plan* plan, const float* d_in, uint in_stride, void* d_iq, void* stream);
 
-/* Delay-and-sum of d_iq [T][C][S] into the complex64 volume d_volume [Z][Y][X]. */
+/* Delay-and-sum of d_iq [T][C][S] into the complex64 volume d_volume [Z][Y][X]. A volume of more
+ * than one wave of tiles (SMs x resident CTAs) is split stream-K style: every CTA takes an equal
+ * share of tiles x stages and the two CTAs that share a tile combine their sums through scratch
+ * memory the plan owns, so calls of one plan must not overlap on the GPU. */
 CUTB_API bool cutb_das(cutb_plan* plan, const void* d_iq, void* d_volume, void* stream);
 
 /* Whole pipeline on device memory, intermediates in the plan's own buffers. */

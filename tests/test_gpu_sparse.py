@@ -32,8 +32,44 @@ def test_network_improves_on_sparse_das(evaluation):
 def test_gate_estimate_tracks_true_nrmse(evaluation):
     _, rows = evaluation
     for r in rows:
-        # a 1/64 tile sample: ~10 % median relative error over 256 held-out volumes
-        assert abs(r["gate_nrmse"] - r["nrmse_net"]) < 0.3 * r["nrmse_net"] + 0.02, r
+        # the network's own volumes sit near NRMSE 0.4, far from the bar: a loose relative check
+        assert abs(r["gate_nrmse"] - r["nrmse_net"]) < 0.1 * r["nrmse_net"], r
+
+
+@pytest.fixture(scope="module")
+def near_bar_cases():
+    """Volumes with a true NRMSE near the 2 % bar, made from real ones: the full-transmit volume V
+    of a held-out phantom plus a fraction of the network's own error, V + lam (V_net - V), and the
+    analytic signal the gate's delay-and-sum reads."""
+    import torch
+    net = sparse.load()
+    path = sparse.LearnedPath(net)
+    cases = []
+    for k in range(3):
+        seed = sparse.EVAL_SEED0 + 100 + k
+        scat = torch.from_numpy(sparse.phantom(seed)).cuda()
+        path.run(scat, seed)
+        iq, gain = path.iq.clone(), path.full.gain.clone()
+        v, vnet = path.vf.clone(), path.vo[0].clone()
+        cases.append((seed, v, vnet - v, iq, gain))
+    return path, cases
+
+
+@pytest.mark.parametrize("target", [0.01, 0.02, 0.03, 0.05])
+def test_gate_is_accurate_near_the_bar(near_bar_cases, target):
+    """Where the gate decides (true NRMSE 1-5 %), its estimate must be within 0.005."""
+    import torch
+    path, cases = near_bar_cases
+    gate, plan = path.gate, path.full.plan
+    for seed, v, err, iq, gain in cases:
+        lam = target * float(torch.linalg.vector_norm(v) / torch.linalg.vector_norm(err))
+        vhat = v + lam * err
+        true = float(torch.linalg.vector_norm(vhat - v) / torch.linalg.vector_norm(v))
+        tiles, w = gate.choose(vhat, seed)
+        vg = plan.das_tiles(iq, tiles, splits=sparse.GATE_SPLITS)
+        vg /= gain
+        est = gate.estimate(vhat, vg, tiles, w)
+        assert abs(est - true) <= 0.005, (seed, target, true, est)
 
 
 def test_rejected_volumes_are_charged_the_fallback(evaluation):
