@@ -59,6 +59,20 @@ constexpr int kSlots = 2 * kBatch;  // metadata ring: a batch never overwrites a
 constexpr float kPi = 3.141592654f;  // value of CUDART_PI_F used upstream
 constexpr long long kWaitLimitCycles = 400000000ll;  // ~0.2 s at 2 GHz
 
+// Template code of tilted plane waves in a y-z plane: the plane-wave delay depends on y, so the
+// tile spans y as for HERCULES. RCA_TPW itself stands for the x-z plane form (y-invariant).
+constexpr int kTpwYz = 100 + RCA_TPW;
+
+// Geometry of each sequence in the staged engine.
+template <int SEQ>
+struct Seq {
+    static constexpr bool kHerc = SEQ == HERCULES;                    // plane/focused transmit, 3-D receive path
+    static constexpr bool kTpw = SEQ == RCA_TPW || SEQ == kTpwYz;     // tilted plane waves, IQ rotation
+    static constexpr bool kUf = SEQ == UFORCES;                       // sparse transmit elements after a flash
+    static constexpr bool kTxPath = SEQ == FORCES || SEQ == UFORCES;  // transmit path from one element
+    static constexpr bool k3d = SEQ == HERCULES || SEQ == kTpwYz;     // voxels of a tile differ in y
+};
+
 // ---- PTX helpers: mbarrier + bulk copy (TMA) ----------------------------------------------
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -162,6 +176,8 @@ struct RowMeta {
     float rx_apo;   // sine receive apodization when it is uniform over the row, else 1
     float loclamp;  // clamp range of the window-relative index: the row's [1, S-2] ...
     float hiclamp;  // ... intersected with the staged window
+    float xc;       // receive element x
+    float rot_c, rot_s;  // TPW: exp(i 2 pi fc/fs lo), the IQ rotation at window index 0
     int lo;         // row sample of window index 0
     int len;        // staged samples; 0: the row is read from global memory
     int unclamped;  // staged, and no voxel of the tile can reach the clamp: the clamp is skipped
@@ -175,8 +191,9 @@ struct StageMeta {
     float two_tx_d0;
     float sign;     // READI sign of this sub-signal
     float uni_apo;  // apodization factor uniform over the stage (sine types)
-    float yj, et;   // receive row y (HERCULES) / transmit element x (FORCES)
-    int t, g, c0, nq;
+    float yj, et;   // receive row y (HERCULES) / transmit element x (FORCES, UFORCES)
+    float s_t, c_t; // TPW: sine and cosine of the plane-wave angle
+    int t, g, c0, nq;  // t: the analytic-signal transmit row (UFORCES: the used transmit + 1)
 };
 
 // Shared memory: NS raw windows per row (TMA destination) and, for NC > 0, one buffer of
@@ -252,6 +269,29 @@ __device__ __forceinline__ StageMeta stage_meta(const DasArgs& a, const StageId&
     }
     s.sign = negate ? -1.f : 1.f;
     s.uni_apo = 1.f;
+    if constexpr (Seq<SEQ>::kTpw) {
+        // plane wave at angle foci[t][2] (radians): delay lat sin(a) + z cos(a), lat = y (y-z plane) or x
+        double sn, cs;
+        sincos((double)a.angles[id.t], &sn, &cs);
+        s.s_t = (float)sn;
+        s.c_t = (float)cs;
+        return s;
+    }
+    if constexpr (Seq<SEQ>::kUf) {
+        // transmit row 0 is the flash: used transmit t reads row t + 1, from element elems[t] -
+        // elems[0] places after the first (the first used transmit is scaled by 1/sqrt(128))
+        s.t = id.t + 1;
+        const double fx = (double)(a.xmin_x + a.px * 0.5f);
+        const double et = fx + (double)(a.elems[id.t] - a.elems[0]) * (double)a.px;
+        const double txd0 = sqrt((tile.cx - et) * (tile.cx - et) + tile.cz * tile.cz);
+        s.et = (float)et;
+        s.tx_d0 = (float)txd0;
+        s.tx_d0sq = (float)(txd0 * txd0);
+        s.two_tx_d0 = (float)(2.0 * txd0);
+        s.ey2 = (float)(-2.0 * (et - tile.cx));
+        s.uni_apo = id.t == 0 ? 0.088388347648318f : 1.f;
+        return s;
+    }
     if (HERC) {
         const double j = a.G > 1 ? (a.encoding == WALSH ? (double)(id.t * a.G + id.g) : (double)(id.g * a.T + id.t))
                                  : (double)id.t;
@@ -286,9 +326,27 @@ __device__ void compute_row(Smem<IQ, NC, DB>& sm, int slot, const StageId& id, i
     RowMeta m{};
     if (q < id.nq) {
         const int c = id.c0 + q;
-        const double xc = (double)a.xmin_x + (double)c * (double)a.px;
+        // receive element: xdc_mins.x + c pitch (HERCULES, FORCES), + pitch / 2 (TPW, UFORCES)
+        const double xc = (double)a.xmin_x + (Seq<SEQ>::kTpw || Seq<SEQ>::kUf ? 0.5 * (double)a.px : 0.0) +
+                          (double)c * (double)a.px;
         double d0, base;
-        if (HERC) {
+        if constexpr (Seq<SEQ>::kTpw) {
+            const double ex = xc - tile.cx;
+            d0 = sqrt(ex * ex + tile.cz * tile.cz);  // the receive path lies in the x-z plane
+            double sn, cs;
+            sincos((double)a.angles[id.t], &sn, &cs);
+            const double lat = SEQ == kTpwYz ? tile.cy : tile.cx;
+            base = (d0 + lat * sn + tile.cz * cs) * (double)a.spm + (double)a.delay;
+            m.ex2 = (float)(-2.0 * ex);
+        } else if constexpr (Seq<SEQ>::kUf) {
+            const double fx = (double)(a.xmin_x + a.px * 0.5f);
+            const double et = fx + (double)(a.elems[id.t] - a.elems[0]) * (double)a.px;
+            const double txd0 = sqrt((tile.cx - et) * (tile.cx - et) + tile.cz * tile.cz);
+            const double ex = xc - tile.cx;
+            d0 = sqrt(ex * ex + tile.cz * tile.cz);
+            base = (txd0 + d0) * (double)a.spm + (double)a.delay;
+            m.ex2 = (float)(-2.0 * ex);
+        } else if (HERC) {
             const double j = a.G > 1 ? (a.encoding == WALSH ? (double)(id.t * a.G + id.g) : (double)(id.g * a.T + id.t))
                                      : (double)id.t;
             const double yj = (double)a.xmin_y + j * (double)a.py;
@@ -624,9 +682,9 @@ struct Layout {
     // four warps stack along z (4 x 8 x 32), or, for SHORT tiles, two along x and two along z
     // (8 x 8 x 16) -- the short tile halves the depth span, and with it the staged window,
     // when the z step is coarse. FORCES: lanes along x (32 x 1 x 32).
-    static constexpr bool kShort = SEQ == HERCULES && SHORT;
-    static constexpr int TX = SEQ == HERCULES ? (kShort ? 8 : 4) : 32;
-    static constexpr int TY = SEQ == HERCULES ? 8 : 1;
+    static constexpr bool kShort = Seq<SEQ>::k3d && SHORT;
+    static constexpr int TX = Seq<SEQ>::k3d ? (kShort ? 8 : 4) : 32;
+    static constexpr int TY = Seq<SEQ>::k3d ? 8 : 1;
     static constexpr int TZ = (kShort ? 2 : kWarps) * kVpt;
 };
 
@@ -954,13 +1012,14 @@ das_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
     das_tile<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>(iq, vol, a, sm, bx, by, bz, k_lo, k_hi);
 }
 
-// Stream-K form of the grid kernel for volumes of more than one wave of tiles: gridDim.x CTAs
-// (one wave: SMs x resident CTAs) split the whole work, tiles x stages, into equal contiguous
-// ranges, so that the last wave is not left partly empty. A CTA walks the tiles of its range in
-// id order (z-major, then y, then x); a tile cut by a range boundary is finished by the second of
-// its two CTAs (the part protocol of das_tile, through a.sk_partials / a.sk_counters). Each range
-// spans at least one tile (gridDim.x <= tiles), so a tile has at most two parts, and the first part
-// of a tile that CTA c cuts lies in c, the last in c + 1: pair c.
+// Stream-K form of the grid kernel for volumes of more than one wave of tiles whose count is not
+// a whole number of waves (gridDim.x CTAs = SMs x resident CTAs, <= tiles). The first waves run as
+// in the grid kernel, CTA c taking tiles c, c + G, ... whole, so that the CTAs of a wave work on
+// neighbouring tiles in step and share their windows in L2. The last wave and the partial one after
+// it (R tiles, G <= R < 2G) are split into G equal contiguous ranges of tiles x stages, so that no
+// CTA idles at the end. A range spans at least one tile, so a tile has at most two parts; the first
+// part of a tile that CTA c cuts lies in c and the last in c + 1 (pair c), and the second to finish
+// adds both (the part protocol of das_tile, through a.sk_partials / a.sk_counters).
 template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT, bool DB>
 __global__ void __launch_bounds__(kThreads, 3)
 das_stream_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
@@ -968,24 +1027,32 @@ das_stream_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a
     extern __shared__ __align__(128) unsigned char smem_raw[];
     auto& sm = *reinterpret_cast<Smem<IQ, coef_arrays<SEQ, CUBIC, APO>(), DB>*>(smem_raw);
     using L = Layout<SEQ, SHORT>;
-    const int nx = div_up(a.X, L::TX), ny = SEQ == HERCULES ? div_up(a.Y, L::TY) : 1;
+    const int nx = div_up(a.X, L::TX), ny = Seq<SEQ>::k3d ? div_up(a.Y, L::TY) : 1;
     const long long nst = tile_stages(a);
-    const long long work = (long long)nx * ny * div_up(a.Z, L::TZ) * nst;
-    const long long s1 = work * (blockIdx.x + 1) / gridDim.x;
-    long long s = work * blockIdx.x / gridDim.x;
-    while (s < s1) {
-        const long long tile = s / nst;
-        const int k0 = (int)(s - tile * nst), k1 = (int)min(nst, s1 - tile * nst);
-        const int part = k0 > 0 ? kPartTail : (k1 < nst ? kPartHead : kPartFull);
-        const int pair = part == kPartTail ? (int)blockIdx.x - 1 : (int)blockIdx.x;
+    const long long ntiles = (long long)nx * ny * div_up(a.Z, L::TZ);
+    const long long G = gridDim.x;
+    const long long whole = (ntiles / G - 1) * G;  // tiles of the data-parallel waves
+    // Runs stages k0 .. k1 - 1 of tile `tile`; false when a bounded wait gave up.
+    auto run = [&](long long tile, int k0, int k1, int part, int pair) {
         das_tile<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>(iq, vol, a, sm, (int)(tile % nx), (int)((tile / nx) % ny),
                                                      (int)(tile / ((long long)nx * ny)), k0, k1, part, pair);
-        s = tile * nst + k1;
         __syncthreads();
-        if (sm.abort[0] | sm.abort[1]) break;
+        if (sm.abort[0] | sm.abort[1]) return false;
         if (threadIdx.x == 0)
             for (int b = 0; b < kStages; ++b) mbar_inval(&sm.full[b]);
         __syncthreads();
+        return true;
+    };
+    for (long long tile = blockIdx.x; tile < whole; tile += G)
+        if (!run(tile, 0, (int)nst, kPartFull, 0)) return;
+    const long long work = (ntiles - whole) * nst;
+    const long long s1 = work * (blockIdx.x + 1) / G;
+    for (long long s = work * blockIdx.x / G; s < s1;) {
+        const long long t = s / nst;
+        const int k0 = (int)(s - t * nst), k1 = (int)min(nst, s1 - t * nst);
+        const int part = k0 > 0 ? kPartTail : (k1 < nst ? kPartHead : kPartFull);
+        if (!run(whole + t, k0, k1, part, part == kPartTail ? (int)blockIdx.x - 1 : (int)blockIdx.x)) return;
+        s = t * nst + k1;
     }
 }
 
@@ -1058,7 +1125,7 @@ bool launch_das_k(const DasArgs& a, const void* iq, void* volume, cudaStream_t s
         if (!wave_size(skern, smem, sk_wave, &wave)) return false;
         const long long tiles = (long long)grid.x * grid.y * grid.z;
         if (g_prepare_only) return true;
-        if (wave > 1 && tiles > wave && tiles % wave != 0 && wave - 1 <= a.sk_capacity) {
+        if (wave > 1 && tiles > wave && (a.schedule == 2 || tiles % wave != 0) && wave - 1 <= a.sk_capacity) {
             CUTB_CUDA_OK(cudaMemsetAsync(a.sk_counters, 0, sizeof(int) * (size_t)wave, st));
             skern<<<wave, kThreads, smem, st>>>((const IQ*)iq, (float2*)volume, a);
             CUTB_CUDA_OK(cudaGetLastError());
@@ -1329,7 +1396,8 @@ void das_tile_shape(const DasArgs& a, int shape[3])
 
 bool prepare_das(const DasArgs& a, bool iq_bf16)
 {
-    if (a.seq != HERCULES && a.seq != FORCES) return true;
+    // sample counts the delay-and-sum rejects are reported at launch
+    if ((a.seq != HERCULES && a.seq != FORCES) || a.S % 4 != 0) return true;
     g_prepare_only = true;
     const bool ok = launch_das(a, nullptr, iq_bf16, nullptr, nullptr, nullptr);
     g_prepare_only = false;

@@ -464,6 +464,9 @@ bool cutb_plan::build(const CudaBeamformerParameters& params, const cutb_options
     CUTB_REQUIRE(opt.das_tile >= 0 && opt.das_tile <= 2, CUTB_ERR_INVALID_ARGUMENT, "Unknown tile id %d.",
                  opt.das_tile);
     das.tile = opt.das_tile;
+    CUTB_REQUIRE(opt.das_schedule >= 0 && opt.das_schedule <= 2, CUTB_ERR_INVALID_ARGUMENT,
+                 "Unknown delay-and-sum schedule %d.", opt.das_schedule);
+    das.schedule = opt.das_schedule;
     if (das.seq == RCA_TPW) {  // beamformer.cu:439-443: angle of transmit t in foci[t][2], radians
         std::vector<float> angles(das.T);
         for (int t = 0; t < das.T; ++t) angles[t] = bp.foci[3 * t + 2];
@@ -490,7 +493,7 @@ bool cutb_plan::build(const CudaBeamformerParameters& params, const cutb_options
         CUTB_CUDA_OK(cudaGetDevice(&dev));
         CUTB_CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         das_grid_tiles(das, counts);
-        if ((long long)counts[0] * counts[1] * counts[2] > sms) {
+        if (das.schedule != 1 && (long long)counts[0] * counts[1] * counts[2] > sms) {
             const int pairs = sms * kStreamPairsPerSm;
             if (!alloc_bytes((void**)&d_sk_partials, sizeof(float4) * 2 * kStreamTileVoxels * (size_t)pairs))
                 return false;

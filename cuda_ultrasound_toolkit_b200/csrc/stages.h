@@ -101,6 +101,7 @@ struct DasArgs {
     const short* elems;        // UFORCES: device transmit element indices (sparse_elements), T entries
     float fc_over_fs;          // RCA_TPW: centre / sampling frequency (IQ rotation)
     int tile;                  // HERCULES tile: 0 chosen from the grid, 1 = 4 x 8 x 32, 2 = 8 x 8 x 16
+    int schedule;              // 0: stream-K for a partial last wave, 1: one CTA per tile, 2: stream-K beyond one wave
     const int* tiles;          // optional device list of tile ids (z-major); null = every tile
     int ntiles;
     int splits;                // > 1: stages split across CTAs, partial sums added atomically

@@ -18,9 +18,11 @@ def main():
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--bf16", action="store_true", help="store the analytic signal as bf16")
     ap.add_argument("--decode-tc", action="store_true", help="decode on int8 tensor cores")
+    ap.add_argument("--schedule", type=int, default=0,
+                    help="delay-and-sum schedule: 0 automatic, 1 one CTA per tile, 2 stream-K")
     args = ap.parse_args()
     raw, bp = synth.frame(args.workload)
-    plan = Plan(bp, iq_bf16=args.bf16, decode_tc=args.decode_tc)
+    plan = Plan(bp, iq_bf16=args.bf16, decode_tc=args.decode_tc, das_schedule=args.schedule)
     d_raw = torch.from_numpy(raw).cuda()
     vol, dec, iq = plan.empty_volume(), plan.empty_decoded(), plan.empty_iq()
     plan.beamform(d_raw, out=vol)

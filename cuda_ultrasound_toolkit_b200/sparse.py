@@ -128,12 +128,28 @@ def make_pairs(n, seed0, log=print):
     return xs, ys
 
 
+def held_out_nrmse(net, xs, ys):
+    """Median and mean NRMSE of the restored volumes net(xs[k]) against ys[k], and of xs itself."""
+    out = torch.empty_like(xs[:1])
+    vals = []
+    for k in range(xs.shape[0]):
+        net.forward(xs[k:k + 1], out=out)
+        vals.append(nrmse(out[0], ys[k]))
+    return float(np.median(vals)), float(np.mean(vals))
+
+
 def train(args, log=print):
     torch.manual_seed(0)
     xs, ys = make_pairs(args.phantoms, TRAIN_SEED0, log)
     net = learn.UNet(GRID, max_batch=args.batch, seed=args.seed)
     steps = args.epochs * (args.phantoms // args.batch)
     gen = torch.Generator(device="cpu").manual_seed(args.seed)
+    curve = []
+    if args.curve:
+        # learning curve: held-out NRMSE after every epoch, on phantoms the training never sees
+        hx, hy = make_pairs(args.curve, EVAL_SEED0 + 500_000, log)
+        base = float(np.median([nrmse(hx[k], hy[k]) for k in range(args.curve)]))
+        log(f"held-out sparse-only NRMSE median {base:.4f}")
     t0, step, hist = time.time(), 0, []
     for ep in range(args.epochs):
         perm = torch.randperm(args.phantoms, generator=gen)
@@ -146,11 +162,22 @@ def train(args, log=print):
                 loss = net.last_loss()
                 hist.append((step, loss))
                 log(f"epoch {ep} step {step}/{steps} loss {loss:.5f} {time.time() - t0:.1f}s")
+        if args.curve:
+            med, mean = held_out_nrmse(net, hx, hy)
+            curve.append((ep + 1, (ep + 1) * args.phantoms, med, mean))
+            log(f"epoch {ep + 1}: held-out NRMSE median {med:.4f} mean {mean:.4f}")
     torch.cuda.synchronize()
     train_s = time.time() - t0
     params = net.get_params()
     np.savez_compressed(args.out, params=params, grid=np.array(GRID), phantoms=args.phantoms, epochs=args.epochs,
-                        batch=args.batch, lr=args.lr, loss=np.array(hist), train_seconds=train_s)
+                        batch=args.batch, lr=args.lr, loss=np.array(hist), train_seconds=train_s,
+                        curve=np.array(curve, dtype=np.float64).reshape(-1, 4))
+    if args.curve:
+        log(json.dumps({"phantoms": args.phantoms, "epochs": args.epochs, "held_out": args.curve,
+                        "sparse_only_nrmse_median": base,
+                        "curve": [dict(epoch=e, phantom_passes=n, nrmse_median=m, nrmse_mean=a)
+                                  for e, n, m, a in curve]}))
+        del hx, hy
     log(f"saved {args.out} ({net.param_count} parameters, {train_s:.1f}s of training)")
     del xs, ys
     return net
@@ -322,6 +349,8 @@ def main():
     t.add_argument("--seed", type=int, default=1)
     t.add_argument("--out", default=WEIGHTS)
     t.add_argument("--eval", type=int, default=0, help="evaluate on this many held-out phantoms afterwards")
+    t.add_argument("--curve", type=int, default=0,
+                   help="held-out phantoms whose NRMSE is logged after every epoch (learning curve)")
     e = sub.add_parser("evaluate")
     e.add_argument("--weights", default=WEIGHTS)
     e.add_argument("--phantoms", type=int, default=256)

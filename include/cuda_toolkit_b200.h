@@ -64,7 +64,10 @@ typedef struct cutb_options {
     int das_tile;     /* delay-and-sum tile: 0 = chosen from the grid, 1 = 4x8x32, 2 = 8x8x16 (HERCULES) */
     int decode_tc;    /* 1: int16 decode on int8 tensor cores (hi/lo byte split, exact); needs 32..256
                          transmits in steps of 32 and rows of 8-sample multiples */
-    int reserved[13];
+    int das_schedule; /* delay-and-sum schedule: 0 = chosen from the grid (stream-K when the tiles are
+                         more than one wave and not a whole number of waves), 1 = one CTA per tile,
+                         2 = stream-K whenever the tiles exceed one wave */
+    int reserved[12];
 } cutb_options;
 
 typedef struct cutb_plan cutb_plan;
