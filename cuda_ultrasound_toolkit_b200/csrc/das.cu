@@ -66,11 +66,9 @@ constexpr int kTpwYz = 100 + RCA_TPW;
 // Geometry of each sequence in the staged engine.
 template <int SEQ>
 struct Seq {
-    static constexpr bool kHerc = SEQ == HERCULES;                    // plane/focused transmit, 3-D receive path
-    static constexpr bool kTpw = SEQ == RCA_TPW || SEQ == kTpwYz;     // tilted plane waves, IQ rotation
-    static constexpr bool kUf = SEQ == UFORCES;                       // sparse transmit elements after a flash
-    static constexpr bool kTxPath = SEQ == FORCES || SEQ == UFORCES;  // transmit path from one element
-    static constexpr bool k3d = SEQ == HERCULES || SEQ == kTpwYz;     // voxels of a tile differ in y
+    static constexpr bool kTpw = SEQ == RCA_TPW || SEQ == kTpwYz;  // tilted plane waves, IQ rotation
+    static constexpr bool kUf = SEQ == UFORCES;                    // sparse transmit elements after a flash
+    static constexpr bool k3d = SEQ == HERCULES || SEQ == kTpwYz;  // voxels of a tile differ in y
 };
 
 // ---- PTX helpers: mbarrier + bulk copy (TMA) ----------------------------------------------
@@ -154,13 +152,13 @@ __device__ __forceinline__ float2 catmull_rom(float2 pm1, float2 p0, float2 p1, 
                        fmaf(h00, p0.y, fmaf(h01, p1.y, fmaf(h10, m0y, h11 * m1y))));
 }
 
-// Guarded read of a global row of n samples; taps past the end read as zero.
+// Guarded read of a global row: row[k] exists for k_min <= k < n; other taps read as zero.
 template <bool CUBIC, class IQ>
-__device__ __forceinline__ float2 interp_global(const IQ* row, float idx, int n)
+__device__ __forceinline__ float2 interp_global(const IQ* row, float idx, int k_min, int n)
 {
     const int i = __float2int_rd(idx);
     const float t = idx - (float)i;
-    auto tap = [&](int k) -> float2 { return k < n ? to_f2(__ldg(row + k)) : make_float2(0.f, 0.f); };
+    auto tap = [&](int k) -> float2 { return k >= k_min && k < n ? to_f2(__ldg(row + k)) : make_float2(0.f, 0.f); };
     if constexpr (CUBIC) return catmull_rom(tap(i - 1), tap(i), tap(i + 1), tap(i + 2), t);
     const float2 p0 = tap(i), p1 = tap(i + 1);
     return make_float2(fmaf(p1.x - p0.x, t, p0.x), fmaf(p1.y - p0.y, t, p0.y));
@@ -373,8 +371,10 @@ __device__ void compute_row(Smem<IQ, NC, DB>& sm, int slot, const StageId& id, i
         // most tile.tx_reach samples.
         const double reach = (double)tile.radius * (double)a.spm + (double)tile.tx_reach + 1.0;
         const double smax = (double)a.S - 2.0;
-        const int i_lo = (int)floor(fmin(fmax(base - reach, 1.0), smax));
-        const int i_hi = (int)floor(fmin(fmax(base + reach, 1.0), smax));
+        // the row clamp: [1, S - 2]; UFORCES [0, S - 2] (its tap below sample 0 reads zero)
+        constexpr int kClampLo = Seq<SEQ>::kUf ? 0 : 1;
+        const int i_lo = (int)floor(fmin(fmax(base - reach, (double)kClampLo), smax));
+        const int i_hi = (int)floor(fmin(fmax(base + reach, (double)kClampLo), smax));
         int lo = max(0, i_lo - 2);
         const int hi = min(a.S, i_hi + 3);          // sample S is a zero tap
         lo -= lo % SA;                               // 16-byte aligned start
@@ -386,11 +386,20 @@ __device__ void compute_row(Smem<IQ, NC, DB>& sm, int slot, const StageId& id, i
         if (a.use_apo && (a.apo_type == RX_TO_SIN || (!HERC && a.apo_type == BOTH_TO_SIN)))
             m.rx_apo = sin_apo((float)xc, a.xmax_x, a.to_power);
         m.lo = lo;
+        m.xc = (float)xc;
+        if constexpr (Seq<SEQ>::kTpw) {  // exp(i 2 pi fc/fs lo), the phase reduced exactly
+            double sn, cs, ph = a.fc_fs * (double)lo;
+            sincospi(2.0 * (ph - floor(ph)), &sn, &cs);
+            m.rot_c = (float)cs;
+            m.rot_s = (float)sn;
+        }
         m.base = (float)(base - (double)lo);
-        m.loclamp = (float)(1 - lo);
+        m.loclamp = (float)(kClampLo - lo);
         m.hiclamp = (float)(a.S - 2 - lo);
         m.len = 0;
-        if (len + SA <= Smem<IQ, NC, DB>::kWin) {
+        // UFORCES stages a row only when no index can come below 1, so the window never needs the
+        // zero tap below sample 0; such rows read the global row with guarded taps instead.
+        if (len + SA <= Smem<IQ, NC, DB>::kWin && (!Seq<SEQ>::kUf || base - reach >= 1.0)) {
             m.len = len;
             m.loclamp = fmaxf(m.loclamp, 1.f);
             m.hiclamp = fminf(m.hiclamp, (float)(len - 3));
@@ -462,9 +471,18 @@ __device__ __forceinline__ float path_offset(float delta, float d0, float d0sq, 
 //
 // Threads first .. first + count - 1 share the items (all threads, or the ones that are not
 // computing window metadata in this stage).
+//
+// rot_tab (TPW): the polynomial of interval i is multiplied by exp(i 2 pi fc/fs (lo + i)), the IQ
+// rotation at its left end, from the row's exp(i 2 pi fc/fs lo) and rot_tab[i] = exp(i 2 pi fc/fs i);
+// a voxel then only rotates by exp(i 2 pi fc/fs t) for its offset t in [0, 1).
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b)
+{
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+
 template <class IQ, int NC, bool DB>
 __device__ __forceinline__ void build_coefficients(Smem<IQ, NC, DB>& sm, int b, int nq, int cb, int wint,
-                                                   float rwint, int first, int count)
+                                                   float rwint, int first, int count, const float2* rot_tab = nullptr)
 {
     if (threadIdx.x < nq) sm.rowc[cb][threadIdx.x] = sm.row[b][threadIdx.x];
     const int n = nq * wint;
@@ -492,6 +510,14 @@ __device__ __forceinline__ void build_coefficients(Smem<IQ, NC, DB>& sm, int b, 
             B.y = fmaf(-0.5f, p2.y, fmaf(2.f, p1.y, fmaf(-2.5f, p0.y, pm1.y)));
             B.z = fmaf(0.5f, p2.x - pm1.x, 1.5f * (p0.x - p1.x));
             B.w = fmaf(0.5f, p2.y - pm1.y, 1.5f * (p0.y - p1.y));
+            if (rot_tab) {
+                const RowMeta& m = sm.row[b][q];
+                const float2 r = cmulf(make_float2(m.rot_c, m.rot_s), rot_tab[i]);
+                const float2 a0 = cmulf(make_float2(A.x, A.y), r), a1 = cmulf(make_float2(A.z, A.w), r);
+                const float2 b0 = cmulf(make_float2(B.x, B.y), r), b1 = cmulf(make_float2(B.z, B.w), r);
+                A = make_float4(a0.x, a0.y, a1.x, a1.y);
+                B = make_float4(b0.x, b0.y, b1.x, b1.y);
+            }
             sm.coefA[cb][q][i] = A;
             sm.coefB[cb][q][i] = B;
         }
@@ -504,16 +530,18 @@ template <int SEQ, bool CUBIC, bool CF, bool APO, bool STAGED, class IQ, int NCS
 __device__ __forceinline__ void row_pass(const DasArgs& a, const Smem<IQ, NCS, DB>& sm, const RowMeta* rows, int b,
                                          int qi, const IQ* grow, const StageMeta& st, float dxe, const float (&sq)[kVpt],
                                          const float (&txs)[kVpt], const float (&vzv)[kVpt], float vx, float a2,
-                                         float2 (&total)[kVpt], float (&inc)[kVpt])
+                                         float2 (&total)[kVpt], float (&inc)[kVpt], const float2* rot_tab = nullptr)
 {
+    using Q = Seq<SEQ>;
     constexpr bool HERC = SEQ == HERCULES;
     constexpr float kMagic = 8388608.f;  // 2^23: adding it with round-down leaves floor(x) in the mantissa
     const RowMeta& m = rows[qi];
     const float exdx = m.ex2 * dxe;
     const float base = m.base, d0 = m.d0, d0sq = m.d0sq, two_d0 = m.two_d0;
     const float loc = m.loclamp, hic = m.hiclamp;
-    float xc = 0.f;
-    if (APO) xc = (float)((double)a.xmin_x + (double)(st.c0 + qi) * (double)a.px);
+    const float xc = m.xc;
+    // TPW: 2 pi fc/fs, for the rotation within an interval
+    const float phi = Q::kTpw ? (float)(6.283185307179586 * a.fc_fs) : 0.f;
 #pragma unroll
     for (int v = 0; v < kVpt; ++v) {
         const float corr = path_offset(exdx + sq[v], d0, d0sq, two_d0);
@@ -521,7 +549,13 @@ __device__ __forceinline__ void row_pass(const DasArgs& a, const Smem<IQ, NCS, D
         if (APO) {
             float apo;
             const float rx = xc - vx;
-            if (HERC) {
+            if constexpr (Q::kTpw || Q::kUf) {
+                // receive Hann window; the windowed value enters both sums (beamformer_kernels.cu:93-172,
+                // 490-550). TPW skips windows below 0.1; UFORCES scales the first transmit by 1/sqrt(128).
+                apo = hann_apo(fabsf(rx), vzv[v], a.fn_rx);
+                if (Q::kTpw && apo < 0.1f) continue;
+                apo *= st.uni_apo;
+            } else if (HERC) {
                 apo = a.apo_type == RX_TO_SIN ? m.rx_apo * st.uni_apo
                                               : hann_apo(sqrtf(fmaf(rx, rx, a2)), vzv[v], a.fn_rx);
                 if (!(apo > 0.1f)) continue;
@@ -553,13 +587,33 @@ __device__ __forceinline__ void row_pass(const DasArgs& a, const Smem<IQ, NCS, D
                 const IQ* p = &sm.raw[b][qi][i];
                 const float2 p0 = to_f2(p[0]), p1 = to_f2(p[1]);
                 val = make_float2(fmaf(p1.x - p0.x, t, p0.x), fmaf(p1.y - p0.y, t, p0.y));
+                // the linear taps are not pre-rotated: rotate to the interval's left end first
+                if constexpr (Q::kTpw) val = cmulf(val, cmulf(make_float2(m.rot_c, m.rot_s), rot_tab[i]));
+            }
+            if constexpr (Q::kTpw) {  // the rest of the rotation, exp(i 2 pi fc/fs t), t in [0, 1)
+                float sn, cs;
+                __sincosf(phi * t, &sn, &cs);
+                val = cmulf(val, make_float2(cs, sn));
             }
         } else {
-            val = interp_global<CUBIC>(grow + m.lo, idx, a.S - m.lo);
+            val = interp_global<CUBIC>(grow + m.lo, idx, -m.lo, a.S - m.lo);
+            if constexpr (Q::kTpw) {  // exp(i 2 pi fc/fs (lo + idx)), the phase reduced in FP64
+                double sn, cs, ph = a.fc_fs * ((double)m.lo + (double)idx);
+                sincospi(2.0 * (ph - floor(ph)), &sn, &cs);
+                val = cmulf(val, make_float2((float)cs, (float)sn));
+            }
         }
-        total[v].x = fmaf(w, val.x, total[v].x);
-        total[v].y = fmaf(w, val.y, total[v].y);
-        if (CF) inc[v] = fmaf(val.x, val.x, fmaf(val.y, val.y, inc[v]));
+        if constexpr (Q::kTpw || Q::kUf) {  // the windowed value enters the incoherent sum
+            val.x *= w;
+            val.y *= w;
+            total[v].x += val.x;
+            total[v].y += val.y;
+            if (CF) inc[v] = fmaf(val.x, val.x, fmaf(val.y, val.y, inc[v]));
+        } else {
+            total[v].x = fmaf(w, val.x, total[v].x);
+            total[v].y = fmaf(w, val.y, total[v].y);
+            if (CF) inc[v] = fmaf(val.x, val.x, fmaf(val.y, val.y, inc[v]));
+        }
     }
 }
 
@@ -706,7 +760,10 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
 {
     constexpr int NC = coef_arrays<SEQ, CUBIC, APO>();
     static_assert(!DB || NC > 0, "two coefficient buffers need coefficients");
+    using Q = Seq<SEQ>;
     constexpr bool HERC = SEQ == HERCULES;
+    constexpr bool Y3 = Q::k3d;  // the tile spans y
+    static_assert(!(Q::kTpw || Q::kUf) || (APO && CF), "TPW and UFORCES always window and weight");
     using L = Layout<SEQ, SHORT>;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
@@ -715,20 +772,20 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
     const float ix_c = tx0 + 0.5f * (L::TX - 1), iy_c = ty0 + 0.5f * (L::TY - 1), iz_c = tz0 + 0.5f * (L::TZ - 1);
     Tile tile;
     tile.cx = (double)a.vmin_x + (double)ix_c * (double)a.res_x;
-    tile.cy = HERC ? (double)a.vmin_y + (double)iy_c * (double)a.res_y : 0.0;
+    tile.cy = Y3 ? (double)a.vmin_y + (double)iy_c * (double)a.res_y : 0.0;
     tile.cz = (double)a.vmin_z + (double)iz_c * (double)a.res_z;
     {
         const double hx = 0.5 * (L::TX - 1) * fabs((double)a.res_x);
-        const double hy = HERC ? 0.5 * (L::TY - 1) * fabs((double)a.res_y) : 0.0;
+        const double hy = Y3 ? 0.5 * (L::TY - 1) * fabs((double)a.res_y) : 0.0;
         const double hz = 0.5 * (L::TZ - 1) * fabs((double)a.res_z);
         tile.radius = (float)(sqrt(hx * hx + hy * hy + hz * hz) * (1.0 + 1e-6) + 1e-9);
     }
-    const int x_idx = tx0 + (HERC ? (L::kShort ? 4 * (warp & 1) : 0) + (lane & 3) : lane);
-    const int y_idx = HERC ? ty0 + (lane >> 2) : 0;
+    const int x_idx = tx0 + (Y3 ? (L::kShort ? 4 * (warp & 1) : 0) + (lane & 3) : lane);
+    const int y_idx = Y3 ? ty0 + (lane >> 2) : 0;
     const int z_first = tz0 + (L::kShort ? (warp >> 1) : warp) * kVpt;
     // Offsets in voxel units are exact in FP32; scaled by the step they carry one rounding.
     const float dxe = ((float)x_idx - ix_c) * a.res_x;
-    const float dye = HERC ? ((float)y_idx - iy_c) * a.res_y : 0.f;
+    const float dye = Y3 ? ((float)y_idx - iy_c) * a.res_y : 0.f;
     const float vx = fmaf((float)x_idx, a.res_x, a.vmin_x);
     const float vy = fmaf((float)y_idx, a.res_y, a.vmin_y);
     float dz[kVpt], vzv[kVpt], txs[kVpt];
@@ -774,11 +831,25 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
                          Smem<IQ, NC, DB>::kWin - 3);
     const float rwint = __frcp_rn((float)wint);
 
-    // |delta|^2 and the z part of -2 (e - centre).delta, per voxel.
+    // |delta|^2 and the z part of -2 (e - centre).delta, per voxel (only HERCULES receive paths
+    // have a y component).
     const float two_cz = (float)(2.0 * tile.cz);
+    const float dyr = HERC ? dye : 0.f;
     float qz[kVpt];
 #pragma unroll
-    for (int v = 0; v < kVpt; ++v) qz[v] = fmaf(two_cz, dz[v], fmaf(dxe, dxe, fmaf(dye, dye, dz[v] * dz[v])));
+    for (int v = 0; v < kVpt; ++v) qz[v] = fmaf(two_cz, dz[v], fmaf(dxe, dxe, fmaf(dyr, dyr, dz[v] * dz[v])));
+
+    // TPW: exp(i 2 pi fc/fs i) for the window indices, formed in FP64 once per tile.
+    const float2* rot_tab = nullptr;
+    if constexpr (Q::kTpw) {
+        __shared__ float2 tpw_rot[Smem<IQ, NC, DB>::kWin];
+        for (int i = threadIdx.x; i < Smem<IQ, NC, DB>::kWin; i += kThreads) {
+            double sn, cs, ph = a.fc_fs * (double)i;
+            sincospi(2.0 * (ph - floor(ph)), &sn, &cs);
+            tpw_rot[i] = make_float2((float)cs, (float)sn);
+        }
+        rot_tab = tpw_rot;  // first read after the barrier that follows the first metadata batch
+    }
 
     // HERCULES without apodization accumulates on packed FP32x2 (row_pass_packed), from cubic or
     // linear coefficients.
@@ -834,8 +905,8 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
         // (j + 1) % kStages, metadata ring slots of stages j + kStages + 1 onwards.
         const int cb = DB ? (j & 1) : 0;
         if constexpr (NC > 0) {
-            if (batch) build_coefficients(sm, b, st.nq, cb, wint, rwint, kMeta, kThreads - kMeta);
-            else build_coefficients(sm, b, st.nq, cb, wint, rwint, 0, kThreads);
+            if (batch) build_coefficients(sm, b, st.nq, cb, wint, rwint, kMeta, kThreads - kMeta, rot_tab);
+            else build_coefficients(sm, b, st.nq, cb, wint, rwint, 0, kThreads, rot_tab);
             all_staged = __syncthreads_and(threadIdx.x >= st.nq || sm.row[b][threadIdx.x].len > 0);
             if (DB && sm.abort[j & 1]) {
                 j_abort = j;
@@ -856,6 +927,9 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
             if (HERC) {
                 sq[v] = fmaf(st.ey2, dye, qz[v]);
                 tsh[v] = txs[v];
+            } else if (Q::kTpw) {  // plane wave: the lateral (y or x) and depth offsets, exact lines
+                sq[v] = qz[v];
+                tsh[v] = fmaf(SEQ == kTpwYz ? dye : dxe, st.s_t, dz[v] * st.c_t) * a.spm;
             } else {
                 sq[v] = qz[v];
                 tsh[v] = path_offset(fmaf(st.ey2, dxe, qz[v]), st.tx_d0, st.tx_d0sq, st.two_tx_d0) * a.spm;
@@ -898,15 +972,15 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
 #pragma unroll 2
             for (int qi = 0; qi < st.nq; ++qi)
                 row_pass<SEQ, CUBIC, CF, APO, true>(a, sm, rows, b, qi, grow0, st, dxe, sq, tsh, vzv, vx, a2, total,
-                                                    inc);
+                                                    inc, rot_tab);
         } else {
             for (int qi = 0; qi < st.nq; ++qi) {
                 if (rows[qi].len > 0)
                     row_pass<SEQ, CUBIC, CF, APO, true>(a, sm, rows, b, qi, grow0, st, dxe, sq, tsh, vzv, vx, a2, total,
-                                                        inc);
+                                                        inc, rot_tab);
                 else
                     row_pass<SEQ, CUBIC, CF, APO, false>(a, sm, rows, b, qi, grow0 + (size_t)qi * a.S, st, dxe, sq, tsh,
-                                                         vzv, vx, a2, total, inc);
+                                                         vzv, vx, a2, total, inc, rot_tab);
             }
         }
         if constexpr (!DB) {
@@ -978,9 +1052,9 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
             float2* o = vol + ((size_t)z * a.Y + y_idx) * a.X + x_idx;
             atomicAdd(&o->x, out.x);
             atomicAdd(&o->y, out.y);
-        } else if (HERC) {
+        } else if (Y3) {
             vol[((size_t)z * a.Y + y_idx) * a.X + x_idx] = out;
-        } else {
+        } else {  // y-invariant: one value for every y
             for (int y = 0; y < a.Y; ++y) vol[((size_t)z * a.Y + y) * a.X + x_idx] = out;
         }
     }
@@ -1032,27 +1106,35 @@ das_stream_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a
     const long long ntiles = (long long)nx * ny * div_up(a.Z, L::TZ);
     const long long G = gridDim.x;
     const long long whole = (ntiles / G - 1) * G;  // tiles of the data-parallel waves
-    // Runs stages k0 .. k1 - 1 of tile `tile`; false when a bounded wait gave up.
-    auto run = [&](long long tile, int k0, int k1, int part, int pair) {
+    const long long work = (ntiles - whole) * nst;
+    const long long s1 = work * (blockIdx.x + 1) / G;
+    long long dp = blockIdx.x, s = work * blockIdx.x / G;
+    // One loop with one call of the (large, inlined) tile body for both phases: two call sites
+    // doubled the code and measured ~40 % slower.
+    for (;;) {
+        long long tile;
+        int k0 = 0, k1 = (int)nst, part = kPartFull, pair = 0;
+        if (dp < whole) {
+            tile = dp;
+            dp += G;
+        } else if (s < s1) {
+            const long long t = s / nst;
+            tile = whole + t;
+            k0 = (int)(s - t * nst);
+            k1 = (int)min(nst, s1 - t * nst);
+            part = k0 > 0 ? kPartTail : (k1 < nst ? kPartHead : kPartFull);
+            pair = part == kPartTail ? (int)blockIdx.x - 1 : (int)blockIdx.x;
+            s = t * nst + k1;
+        } else {
+            break;
+        }
         das_tile<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>(iq, vol, a, sm, (int)(tile % nx), (int)((tile / nx) % ny),
                                                      (int)(tile / ((long long)nx * ny)), k0, k1, part, pair);
         __syncthreads();
-        if (sm.abort[0] | sm.abort[1]) return false;
+        if (sm.abort[0] | sm.abort[1]) return;
         if (threadIdx.x == 0)
             for (int b = 0; b < kStages; ++b) mbar_inval(&sm.full[b]);
         __syncthreads();
-        return true;
-    };
-    for (long long tile = blockIdx.x; tile < whole; tile += G)
-        if (!run(tile, 0, (int)nst, kPartFull, 0)) return;
-    const long long work = (ntiles - whole) * nst;
-    const long long s1 = work * (blockIdx.x + 1) / G;
-    for (long long s = work * blockIdx.x / G; s < s1;) {
-        const long long t = s / nst;
-        const int k0 = (int)(s - t * nst), k1 = (int)min(nst, s1 - t * nst);
-        const int part = k0 > 0 ? kPartTail : (k1 < nst ? kPartHead : kPartFull);
-        if (!run(whole + t, k0, k1, part, part == kPartTail ? (int)blockIdx.x - 1 : (int)blockIdx.x)) return;
-        s = t * nst + k1;
     }
 }
 
@@ -1109,7 +1191,7 @@ bool launch_das_k(const DasArgs& a, const void* iq, void* volume, cudaStream_t s
 {
     using L = Layout<SEQ, SHORT>;
     // FORCES does not depend on y: one y-slice of tiles, each written to every y.
-    dim3 grid(div_up(a.X, L::TX), SEQ == HERCULES ? div_up(a.Y, L::TY) : 1, div_up(a.Z, L::TZ));
+    dim3 grid(div_up(a.X, L::TX), Seq<SEQ>::k3d ? div_up(a.Y, L::TY) : 1, div_up(a.Z, L::TZ));
     if (a.tiles) grid = dim3(a.ntiles, a.splits > 1 ? a.splits : 1, 1);
     CUTB_REQUIRE(grid.y <= 65535 && grid.z <= 65535, CUTB_ERR_UNSUPPORTED, "Output grid too large.");
     auto kern = das_kernel<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>;
@@ -1125,7 +1207,7 @@ bool launch_das_k(const DasArgs& a, const void* iq, void* volume, cudaStream_t s
         if (!wave_size(skern, smem, sk_wave, &wave)) return false;
         const long long tiles = (long long)grid.x * grid.y * grid.z;
         if (g_prepare_only) return true;
-        if (wave > 1 && tiles > wave && (a.schedule == 2 || tiles % wave != 0) && wave - 1 <= a.sk_capacity) {
+        if (a.schedule == 2 && wave > 1 && tiles > wave && wave - 1 <= a.sk_capacity) {
             CUTB_CUDA_OK(cudaMemsetAsync(a.sk_counters, 0, sizeof(int) * (size_t)wave, st));
             skern<<<wave, kThreads, smem, st>>>((const IQ*)iq, (float2*)volume, a);
             CUTB_CUDA_OK(cudaGetLastError());
@@ -1175,6 +1257,14 @@ bool prefer_short_tile(const DasArgs& a)
     const double hz = 15.5 * std::fabs((double)a.res_z);
     const double reach = std::sqrt(hx * hx + hy * hy + hz * hz) * (double)a.spm;
     return 4.0 * reach + 8.0 > (double)(kWinMax - 8);
+}
+
+// TPW and UFORCES: always windowed, always weighted by the coherence factor.
+template <int SEQ, class IQ, bool SHORT>
+bool launch_das_seq(const DasArgs& a, const void* iq, void* volume, cudaStream_t st)
+{
+    if (a.cubic) return launch_das_k<SEQ, true, true, true, IQ, SHORT, false>(a, iq, volume, st);
+    return launch_das_k<SEQ, false, true, true, IQ, SHORT, false>(a, iq, volume, st);
 }
 
 template <int SEQ, class IQ, bool SHORT>
@@ -1262,6 +1352,7 @@ bool derive_das(const CudaBeamformerParameters& bp, DasArgs& a)
     }
 
     a.fc_over_fs = bp.center_frequency / bp.sampling_frequency;
+    a.fc_fs = (double)bp.center_frequency / (double)bp.sampling_frequency;
     if (a.seq == RCA_TPW || a.seq == UFORCES) {
         // beamformer.cu:161-189, 416-468: no READI; TPW needs a plane focus, UFORCES the
         // sparse-element table (and, for a defined transmit path, a focus in the x-z plane).
@@ -1319,9 +1410,19 @@ bool derive_das(const CudaBeamformerParameters& bp, DasArgs& a)
     return true;
 }
 
+// Sequences whose voxels differ in y within a tile: HERCULES, and tilted plane waves in a y-z plane.
+static bool das_3d(const DasArgs& a) { return a.seq == HERCULES || (a.seq == RCA_TPW && a.focus == 2); }
+// TPW and UFORCES on the one-thread-per-voxel kernel (das_direct.cu) instead of the staged engine.
+static bool das_direct(const DasArgs& a) { return (a.seq == RCA_TPW || a.seq == UFORCES) && a.tile == 3; }
+
 static bool use_short_tile(const DasArgs& a)
 {
-    return a.seq == HERCULES && (a.tile == 2 || (a.tile == 0 && prefer_short_tile(a)));
+    return das_3d(a) && (a.tile == 2 || (a.tile == 0 && prefer_short_tile(a)));
+}
+
+bool das_staged(const DasArgs& a)
+{
+    return (a.seq == HERCULES || a.seq == FORCES || a.seq == RCA_TPW || a.seq == UFORCES) && !das_direct(a);
 }
 
 bool das_uses_short_tile(const DasArgs& a) { return use_short_tile(a); }
@@ -1383,21 +1484,21 @@ void das_grid_tiles(const DasArgs& a, int counts[3])
     int shape[3];
     das_tile_shape(a, shape);
     for (int i = 0; i < 3; ++i) counts[i] = div_up(i == 0 ? a.X : i == 1 ? a.Y : a.Z, shape[i]);
-    if (a.seq != HERCULES) counts[1] = 1;  // y-invariant: one slice of tiles
+    if (!das_3d(a)) counts[1] = 1;  // y-invariant: one slice of tiles
 }
 
 void das_tile_shape(const DasArgs& a, int shape[3])
 {
     const bool sh = use_short_tile(a);
-    shape[0] = a.seq == HERCULES ? (sh ? Layout<HERCULES, true>::TX : Layout<HERCULES, false>::TX) : Layout<FORCES, false>::TX;
-    shape[1] = a.seq == HERCULES ? 8 : 1;
+    shape[0] = das_3d(a) ? (sh ? Layout<HERCULES, true>::TX : Layout<HERCULES, false>::TX) : Layout<FORCES, false>::TX;
+    shape[1] = das_3d(a) ? 8 : 1;
     shape[2] = sh ? Layout<HERCULES, true>::TZ : Layout<HERCULES, false>::TZ;
 }
 
 bool prepare_das(const DasArgs& a, bool iq_bf16)
 {
     // sample counts the delay-and-sum rejects are reported at launch
-    if ((a.seq != HERCULES && a.seq != FORCES) || a.S % 4 != 0) return true;
+    if (!das_staged(a) || a.S % 4 != 0) return true;
     g_prepare_only = true;
     const bool ok = launch_das(a, nullptr, iq_bf16, nullptr, nullptr, nullptr);
     g_prepare_only = false;
@@ -1414,8 +1515,23 @@ bool launch_das(const DasArgs& a, const void* iq, bool iq_bf16, void* volume, cu
     bool ok;
     if (a.seq == RCA_TPW || a.seq == UFORCES) {
         CUTB_REQUIRE(!a.tiles, CUTB_ERR_UNSUPPORTED, "Tile lists need HERCULES.");
-        const bool ok = launch_das_direct(a, iq, iq_bf16, volume, st);
-        if (ok && launches) ++*launches;
+        if (das_direct(a)) {
+            if (g_prepare_only) return true;
+            ok = launch_das_direct(a, iq, iq_bf16, volume, st);
+        } else if (a.seq == UFORCES) {
+            ok = iq_bf16 ? launch_das_seq<UFORCES, __nv_bfloat162, false>(a, iq, volume, st)
+                         : launch_das_seq<UFORCES, float2, false>(a, iq, volume, st);
+        } else if (a.focus != 2) {  // plane waves in the x-z plane: y-invariant
+            ok = iq_bf16 ? launch_das_seq<RCA_TPW, __nv_bfloat162, false>(a, iq, volume, st)
+                         : launch_das_seq<RCA_TPW, float2, false>(a, iq, volume, st);
+        } else if (use_short_tile(a)) {
+            ok = iq_bf16 ? launch_das_seq<kTpwYz, __nv_bfloat162, true>(a, iq, volume, st)
+                         : launch_das_seq<kTpwYz, float2, true>(a, iq, volume, st);
+        } else {
+            ok = iq_bf16 ? launch_das_seq<kTpwYz, __nv_bfloat162, false>(a, iq, volume, st)
+                         : launch_das_seq<kTpwYz, float2, false>(a, iq, volume, st);
+        }
+        if (ok && launches && !g_prepare_only) ++*launches;
         return ok;
     }
     CUTB_REQUIRE(!a.tiles || (a.ntiles > 0 && a.ntiles <= (1 << 24)), CUTB_ERR_INVALID_ARGUMENT, "Bad tile list.");

@@ -405,8 +405,8 @@ CUTB_API bool cutb_debug_das_skip_stage(cutb_plan* p, int stage, long long wait_
     CUTB_REQUIRE(p, CUTB_ERR_INVALID_ARGUMENT, "Null plan.");
     CUTB_REQUIRE(stage >= -1 && wait_limit_cycles >= 0, CUTB_ERR_INVALID_ARGUMENT,
                  "Stage must be -1 (off) or a stage index, the wait limit non-negative.");
-    CUTB_REQUIRE(p->das.seq == HERCULES || p->das.seq == FORCES, CUTB_ERR_UNSUPPORTED,
-                 "Only the staged (HERCULES / FORCES) delay-and-sum has bounded waits.");
+    CUTB_REQUIRE(das_staged(p->das), CUTB_ERR_UNSUPPORTED,
+                 "Only the staged delay-and-sum has bounded waits (not the one-thread-per-voxel kernel).");
     p->das.debug_skip = stage + 1;
     p->das.wait_limit = wait_limit_cycles;
     return true;
@@ -461,8 +461,10 @@ bool cutb_plan::build(const CudaBeamformerParameters& params, const cutb_options
         return false;
     }
     if (!derive_das(bp, das)) return false;
-    CUTB_REQUIRE(opt.das_tile >= 0 && opt.das_tile <= 2, CUTB_ERR_INVALID_ARGUMENT, "Unknown tile id %d.",
+    CUTB_REQUIRE(opt.das_tile >= 0 && opt.das_tile <= 3, CUTB_ERR_INVALID_ARGUMENT, "Unknown tile id %d.",
                  opt.das_tile);
+    CUTB_REQUIRE(opt.das_tile != 3 || das.seq == RCA_TPW || das.seq == UFORCES, CUTB_ERR_INVALID_ARGUMENT,
+                 "The one-thread-per-voxel delay-and-sum (tile 3) serves TPW and UFORCES.");
     das.tile = opt.das_tile;
     CUTB_REQUIRE(opt.das_schedule >= 0 && opt.das_schedule <= 2, CUTB_ERR_INVALID_ARGUMENT,
                  "Unknown delay-and-sum schedule %d.", opt.das_schedule);
@@ -487,13 +489,13 @@ bool cutb_plan::build(const CudaBeamformerParameters& params, const cutb_options
     CUTB_CUDA_OK(cudaMemset(d_status, 0, sizeof(int)));
     das.status = d_status;
     if (opt.decode_tc && !fe.enable_tc_decode(d_status)) return false;
-    if (das.seq == HERCULES || das.seq == FORCES) {
+    if (das_staged(das)) {
         // Stream-K scratch of the staged delay-and-sum, for volumes of more than one wave of tiles.
         int dev = 0, sms = 0, counts[3];
         CUTB_CUDA_OK(cudaGetDevice(&dev));
         CUTB_CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         das_grid_tiles(das, counts);
-        if (das.schedule != 1 && (long long)counts[0] * counts[1] * counts[2] > sms) {
+        if (das.schedule == 2 && (long long)counts[0] * counts[1] * counts[2] > sms) {
             const int pairs = sms * kStreamPairsPerSm;
             if (!alloc_bytes((void**)&d_sk_partials, sizeof(float4) * 2 * kStreamTileVoxels * (size_t)pairs))
                 return false;

@@ -100,8 +100,10 @@ struct DasArgs {
     const float* angles;       // RCA_TPW: device plane-wave angles (foci[t][2]), T entries
     const short* elems;        // UFORCES: device transmit element indices (sparse_elements), T entries
     float fc_over_fs;          // RCA_TPW: centre / sampling frequency (IQ rotation)
-    int tile;                  // HERCULES tile: 0 chosen from the grid, 1 = 4 x 8 x 32, 2 = 8 x 8 x 16
-    int schedule;              // 0: stream-K for a partial last wave, 1: one CTA per tile, 2: stream-K beyond one wave
+    double fc_fs;              // the same ratio formed in FP64 from the FP32 frequencies
+    int tile;                  // 0 chosen from the grid, 1 = 4 x 8 x 32, 2 = 8 x 8 x 16 (HERCULES, TPW in a
+                               // y-z plane), 3 = one thread per voxel (TPW, UFORCES)
+    int schedule;              // 0, 1: one CTA per tile; 2: stream-K beyond one wave
     const int* tiles;          // optional device list of tile ids (z-major); null = every tile
     int ntiles;
     int splits;                // > 1: stages split across CTAs, partial sums added atomically
@@ -133,6 +135,8 @@ static_assert(sizeof(DasBatchParams) <= 32000, "batched delay-and-sum parameter 
 bool launch_das_batch(const DasBatchParams* P, const int2* items, int nitems, int* counter, const DasArgs& like,
                       bool iq_bf16, bool short_tile, int grid, int* per_sm, cudaStream_t st);
 bool das_uses_short_tile(const DasArgs& a);
+// True when the delay-and-sum of `a` runs on the staged (TMA window) engine with bounded waits.
+bool das_staged(const DasArgs& a);
 // Tiles along x, y, z of the delay-and-sum grid for these arguments.
 void das_grid_tiles(const DasArgs& a, int counts[3]);
 

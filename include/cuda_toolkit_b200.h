@@ -61,12 +61,15 @@ CUTB_API bool cutb_encoding_matrix(uint n, int ordering, signed char* out);
 /* Options that the parameter struct has no field for. Zero-initialise for defaults. */
 typedef struct cutb_options {
     int iq_bf16;      /* 1: analytic signal stored as bf16 complex (halves DAS gather bytes) */
-    int das_tile;     /* delay-and-sum tile: 0 = chosen from the grid, 1 = 4x8x32, 2 = 8x8x16 (HERCULES) */
+    int das_tile;     /* delay-and-sum tile: 0 = chosen from the grid, 1 = 4x8x32, 2 = 8x8x16 (HERCULES and
+                         TPW in a y-z plane), 3 = one thread per voxel instead of the staged engine
+                         (TPW and UFORCES only) */
     int decode_tc;    /* 1: int16 decode on int8 tensor cores (hi/lo byte split, exact); needs 32..256
                          transmits in steps of 32 and rows of 8-sample multiples */
-    int das_schedule; /* delay-and-sum schedule: 0 = chosen from the grid (stream-K when the tiles are
-                         more than one wave and not a whole number of waves), 1 = one CTA per tile,
-                         2 = stream-K whenever the tiles exceed one wave */
+    int das_schedule; /* delay-and-sum schedule: 0 = default (one CTA per tile), 1 = one CTA per tile,
+                         2 = stream-K when the tiles exceed one wave: the last waves' tiles x stages
+                         split evenly over the resident CTAs, partial sums combined through plan-owned
+                         scratch memory */
     int reserved[12];
 } cutb_options;
 
@@ -95,10 +98,10 @@ CUTB_API bool cutb_decode(cutb_plan* plan, const void* d_raw, size_t raw_bytes, 
  * CUTB_ERR_UNSUPPORTED. */
 CUTB_API bool cutb_hilbert(cutb_plan* plan, const float* d_in, uint in_stride, void* d_iq, void* stream);
 
-/* Delay-and-sum of d_iq [T][C][S] into the complex64 volume d_volume [Z][Y][X]. A volume of more
- * than one wave of tiles (SMs x resident CTAs) is split stream-K style: every CTA takes an equal
- * share of tiles x stages and the two CTAs that share a tile combine their sums through scratch
- * memory the plan owns, so calls of one plan must not overlap on the GPU. */
+/* Delay-and-sum of d_iq [T][C][S] into the complex64 volume d_volume [Z][Y][X]. With
+ * das_schedule = 2 a volume of more than one wave of tiles (SMs x resident CTAs) is split stream-K
+ * style and the two CTAs that share a tile combine their sums through scratch memory the plan
+ * owns; calls of one plan must then not overlap on the GPU. */
 CUTB_API bool cutb_das(cutb_plan* plan, const void* d_iq, void* d_volume, void* stream);
 
 /* Whole pipeline on device memory, intermediates in the plan's own buffers. */
@@ -143,12 +146,13 @@ CUTB_API int cutb_batch_das_launches(const cutb_batch* batch);
  * wait (CUTB_ERR_TIMEOUT); clears the flag. cuda_toolkit::beamform calls it on every frame. */
 CUTB_API bool cutb_plan_check(cutb_plan* plan, void* stream);
 
-/* Test hook for the bounded waits of the staged delay-and-sum (HERCULES / FORCES): from the next
+/* Test hook for the bounded waits of the staged delay-and-sum: from the next
  * call on, stage `stage` (transmit x channel-group step, counted from 0 in every CTA) is never
  * issued, so the wait for its copies runs out after wait_limit_cycles (0: the default of about
  * 0.2 s), the CTA stops, waits for the copies it had already issued and leaves; cutb_plan_check
  * then reports CUTB_ERR_TIMEOUT. stage = -1 turns the hook off. The volume of such a call is
- * undefined. No GPU fault is involved: every wait stays bounded. */
+ * undefined. No GPU fault is involved: every wait stays bounded. Every sequence runs on the staged
+ * engine except TPW / UFORCES plans created with das_tile = 3, which are rejected here. */
 CUTB_API bool cutb_debug_das_skip_stage(cutb_plan* plan, int stage, long long wait_limit_cycles);
 
 /* Number of kernels the last cutb_beamform/cutb_decode/cutb_hilbert/cutb_das call launched. */

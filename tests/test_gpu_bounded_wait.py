@@ -37,13 +37,27 @@ def params(kind):
     if kind == "forces":
         bp.das_shader_id = int(SequenceId.FORCES)
         bp.tx_orientation = bp.rx_orientation
+    if kind in ("tpw_xz", "tpw_yz"):
+        bp.das_shader_id = int(SequenceId.RCA_TPW)
+        if kind == "tpw_xz":
+            bp.tx_orientation = bp.rx_orientation
+        for t, ang in enumerate(np.linspace(-0.2, 0.2, T)):
+            bp.foci[3 * t + 2] = float(ang)
+    if kind == "uforces":
+        bp.das_shader_id = int(SequenceId.UFORCES)
+        bp.tx_orientation = bp.rx_orientation
+        bp.foci[2] = 10e-3
+        for t in range(T):
+            bp.sparse_elements[t] = t
     return bp
 
 
 # default: short tile with double-buffered coefficients; long: 4 x 8 x 32 tile, one coefficient
 # buffer; apo: apodized cubic (scalar row pass); linear: packed linear coefficients; linear_apo:
-# raw taps, no coefficients; forces: the y-invariant sequence.
-CASES = [("default", 0), ("long", 1), ("apo", 0), ("linear", 0), ("linear_apo", 0), ("forces", 0)]
+# raw taps, no coefficients; forces: the y-invariant sequence; tpw_xz / tpw_yz: tilted plane waves
+# (y-invariant, and over y); uforces: sparse transmit elements after a flash.
+CASES = [("default", 0), ("long", 1), ("apo", 0), ("linear", 0), ("linear_apo", 0), ("forces", 0),
+         ("tpw_xz", 0), ("tpw_yz", 0), ("uforces", 0)]
 
 
 @pytest.mark.parametrize("kind,tile", CASES)
@@ -52,7 +66,7 @@ def test_missing_stage_times_out_and_plan_recovers(torch, kind, tile, where):
     bp = params(kind)
     plan = Plan(bp, das_tile=tile)
     S, C, T = bp.dims
-    stages = T * ((C + 7) // 8)
+    stages = (T - (kind == "uforces")) * ((C + 7) // 8)  # UFORCES: transmit row 0 is the flash
     stage = {"first": 0, "middle": stages // 2 + 1, "last": stages - 1}[where]
     g = torch.Generator(device="cuda").manual_seed(5)
     iq = torch.complex(torch.randn(T, C, S, device="cuda", generator=g),
@@ -73,11 +87,11 @@ def test_missing_stage_times_out_and_plan_recovers(torch, kind, tile, where):
     assert torch.equal(vol, ref)
 
 
-def test_skip_stage_rejects_sequences_without_waits(torch):
+def test_skip_stage_rejects_kernels_without_waits(torch):
     bp = params("default")
     bp.das_shader_id = int(SequenceId.RCA_TPW)
     bp.tx_orientation = bp.rx_orientation
-    plan = Plan(bp)
+    plan = Plan(bp, das_tile=3)  # one thread per voxel: no staged copies, no waits
     with pytest.raises(CutbError):
         plan.debug_skip_stage(0, WAIT_LIMIT)
 

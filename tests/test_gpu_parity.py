@@ -280,7 +280,8 @@ TPW_UFORCES_CASES = [
 @pytest.mark.parametrize("case", TPW_UFORCES_CASES, ids=lambda c: f"{int(c['seq'])}-" + "-".join(
     f"{k}" for k in c if k != "seq"))
 @pytest.mark.parametrize("bf16", [False, True])
-def test_das_tpw_uforces_vs_fp64(torch, orc, case, bf16):
+@pytest.mark.parametrize("tile", [0, 1, 3])  # staged engine (chosen / 4 x 8 x 32 tile), one thread per voxel
+def test_das_tpw_uforces_vs_fp64(torch, orc, case, bf16, tile):
     case = dict(case)
     angles, elems, same = case.pop("angles", None), case.pop("elems", None), case.pop("same", False)
     bp = das_params(**case)
@@ -294,7 +295,7 @@ def test_das_tpw_uforces_vs_fp64(torch, orc, case, bf16):
             bp.sparse_elements[t] = int(e)
     S, C, T = bp.dims
     iq = analytic_rows(orc, T, C, S, seed=21 + len(str(case)))
-    plan = Plan(bp, iq_bf16=bf16)
+    plan = Plan(bp, iq_bf16=bf16, das_tile=tile)
     if bf16:
         d = torch.from_numpy(np.stack([iq.real, iq.imag], -1).astype(np.float32)).cuda().to(torch.bfloat16)
     else:
