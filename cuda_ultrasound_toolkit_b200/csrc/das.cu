@@ -36,6 +36,7 @@
 //   * a single output point along x or z gets step 0 (upstream divides by zero);
 //   * FORCES does not depend on y (upstream recomputes every y): one y-slice is computed
 //     and written to every y.
+#include <algorithm>
 #include <cmath>
 
 #include <cuda_bf16.h>
@@ -744,19 +745,25 @@ struct Layout {
 
 // Parts of a tile under the stream-K decomposition (das_stream_kernel): the whole stage range, or
 // the first or the last part of a tile whose stages two consecutive CTAs share.
-constexpr int kPartFull = 0, kPartHead = 1, kPartTail = 2;
+// kPartSplit: part `pair` of `nparts` equal stage slices of tile `tile_id` (das_split_kernel).
+constexpr int kPartFull = 0, kPartHead = 1, kPartTail = 2, kPartSplit = 3;
 constexpr int kTileVoxels = kThreads * kVpt;
 static_assert(kTileVoxels == (int)kStreamTileVoxels, "stream-K scratch holds one record per voxel of a tile");
 
-// Stages of one tile: transmits x channel groups x READI sub-signals.
-__host__ __device__ __forceinline__ int tile_stages(const DasArgs& a) { return a.T * div_up(a.C, kRows) * a.G; }
+// Stages of one tile: transmits x channel groups x READI sub-signals. UFORCES sums T - 1 transmits
+// (row 0 is the flash; used transmit t reads row t + 1).
+__host__ __device__ __forceinline__ int tile_stages(const DasArgs& a)
+{
+    return (a.seq == UFORCES ? a.T - 1 : a.T) * div_up(a.C, kRows) * a.G;
+}
 
 // One tile (bx, by, bz) of the volume, stages k_lo .. k_hi - 1. Called by the grid
 // kernel (a in parameter space) and by the persistent batch kernel (a in its parameter table).
 template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT, bool DB = false>
 __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __restrict__ vol, const DasArgs& a,
                                          Smem<IQ, coef_arrays<SEQ, CUBIC, APO>(), DB>& sm, int bx, int by, int bz,
-                                         int k_lo, int k_hi, int part = kPartFull, int pair = 0)
+                                         int k_lo, int k_hi, int part = kPartFull, int pair = 0, int nparts = 1,
+                                         int tile_id = 0)
 {
     constexpr int NC = coef_arrays<SEQ, CUBIC, APO>();
     static_assert(!DB || NC > 0, "two coefficient buffers need coefficients");
@@ -1012,7 +1019,36 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
             inc[v] += ix + iy;
         }
     }
-    if (part != kPartFull) {
+    if (part == kPartSplit) {
+        // Split: nparts CTAs summed equal stage slices of this tile. Each writes its sums to its own
+        // record and counts its arrival; the last to arrive adds all records in slice order (its own
+        // read back too), so the result does not depend on the arrival order. Nothing waits.
+        float4* rec = a.sk_partials + (size_t)tile_id * nparts * kTileVoxels;
+#pragma unroll
+        for (int v = 0; v < kVpt; ++v)
+            rec[(size_t)pair * kTileVoxels + threadIdx.x * kVpt + v] = make_float4(total[v].x, total[v].y, inc[v], 0.f);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) sm.part_last = atomicAdd(a.sk_counters + tile_id, 1);
+        __syncthreads();
+        if (sm.part_last != nparts - 1) return;  // a later slice finishes the tile
+        __threadfence();
+#pragma unroll
+        for (int v = 0; v < kVpt; ++v) {
+            total[v] = make_float2(0.f, 0.f);
+            inc[v] = 0.f;
+        }
+        for (int p = 0; p < nparts; ++p) {
+#pragma unroll
+            for (int v = 0; v < kVpt; ++v) {
+                const float4 o = __ldcg(rec + (size_t)p * kTileVoxels + threadIdx.x * kVpt + v);
+                total[v].x += o.x;
+                total[v].y += o.y;
+                inc[v] += o.z;
+            }
+        }
+        if (threadIdx.x == 0) a.sk_counters[tile_id] = 0;  // ready for the next launch
+    } else if (part != kPartFull) {
         // Stream-K: two consecutive CTAs summed the two parts of this tile's stages. Each writes its
         // sums to its own slot of the pair's scratch, then counts its arrival; the second to arrive
         // adds the other part's sums and finishes the tile. Addition of the two parts commutes, so
@@ -1138,6 +1174,25 @@ das_stream_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a
     }
 }
 
+// Split form for volumes of fewer tiles than half a wave (small 2-D slices of the y-invariant
+// sequences): CTA (blockIdx.x, blockIdx.y) sums stage slice blockIdx.y of gridDim.y of tile
+// blockIdx.x (id order: z-major, then y, then x), and the last slice to finish a tile adds all
+// slices (the kPartSplit protocol of das_tile, through a.sk_partials / a.sk_counters).
+template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT, bool DB>
+__global__ void __launch_bounds__(kThreads, 3)
+das_split_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    auto& sm = *reinterpret_cast<Smem<IQ, coef_arrays<SEQ, CUBIC, APO>(), DB>*>(smem_raw);
+    using L = Layout<SEQ, SHORT>;
+    const int nx = div_up(a.X, L::TX), ny = Seq<SEQ>::k3d ? div_up(a.Y, L::TY) : 1;
+    const int tile = blockIdx.x, P = gridDim.y, p = blockIdx.y;
+    const long long nst = tile_stages(a);
+    das_tile<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>(iq, vol, a, sm, tile % nx, (tile / nx) % ny, tile / (nx * ny),
+                                                 (int)(nst * p / P), (int)(nst * (p + 1) / P), kPartSplit, p, P,
+                                                 tile);
+}
+
 // Persistent delay-and-sum over the tiles of many frames: CTAs take (frame, tile) work items,
 // heaviest first, from a device counter until the list is exhausted. Frame arguments sit in the
 // kernel's parameter table (uniform per CTA, read through the constant cache).
@@ -1196,6 +1251,27 @@ bool launch_das_k(const DasArgs& a, const void* iq, void* volume, cudaStream_t s
     CUTB_REQUIRE(grid.y <= 65535 && grid.z <= 65535, CUTB_ERR_UNSUPPORTED, "Output grid too large.");
     auto kern = das_kernel<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>;
     const size_t smem = sizeof(Smem<IQ, coef_arrays<SEQ, CUBIC, APO>(), DB>);
+    if (!a.tiles && a.sk_partials && a.sk_counters && SEQ != HERCULES) {
+        // Fewer tiles than half a wave: split every tile's stages over P CTAs (at least 8 stages
+        // each) so that the volume still fills the GPU.
+        auto pkern = das_split_kernel<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>;
+        static std::atomic<uint64_t> sp_smem_set{0};
+        static std::atomic<int> sp_wave[64];
+        if (!set_smem_limit(pkern, smem, sp_smem_set)) return false;
+        int wave = 0;
+        if (!wave_size(pkern, smem, sp_wave, &wave)) return false;
+        const long long tiles = (long long)grid.x * grid.y * grid.z;
+        const long long P = std::min<long long>(std::min<long long>(wave / std::max<long long>(tiles, 1),
+                                                                    tile_stages(a) / kBatch),
+                                                2LL * a.sk_capacity / std::max<long long>(tiles, 1));
+        if (g_prepare_only) return true;
+        if (2 * tiles <= wave && P >= 2 && tiles <= a.sk_capacity) {
+            CUTB_CUDA_OK(cudaMemsetAsync(a.sk_counters, 0, sizeof(int) * (size_t)tiles, st));
+            pkern<<<dim3((unsigned)tiles, (unsigned)P), kThreads, smem, st>>>((const IQ*)iq, (float2*)volume, a);
+            CUTB_CUDA_OK(cudaGetLastError());
+            return true;
+        }
+    }
     if (!a.tiles && a.sk_partials && a.sk_counters) {
         // More than one wave of tiles that is not a whole number of waves: the stream-K form
         // spreads the last, partly empty wave's work over every CTA.

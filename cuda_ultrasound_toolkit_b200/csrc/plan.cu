@@ -490,12 +490,15 @@ bool cutb_plan::build(const CudaBeamformerParameters& params, const cutb_options
     das.status = d_status;
     if (opt.decode_tc && !fe.enable_tc_decode(d_status)) return false;
     if (das_staged(das)) {
-        // Stream-K scratch of the staged delay-and-sum, for volumes of more than one wave of tiles.
+        // Scratch of the staged delay-and-sum for partial sums of tiles split over several CTAs.
         int dev = 0, sms = 0, counts[3];
         CUTB_CUDA_OK(cudaGetDevice(&dev));
         CUTB_CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         das_grid_tiles(das, counts);
-        if (das.schedule == 2 && (long long)counts[0] * counts[1] * counts[2] > sms) {
+        const long long tiles = (long long)counts[0] * counts[1] * counts[2];
+        // stream-K (HERCULES on request) beyond one wave; the split form for small volumes of the
+        // other sequences (fewer tiles than half a wave)
+        if ((das.schedule == 2 && tiles > sms) || (das.seq != HERCULES && 2 * tiles <= 3LL * sms)) {
             const int pairs = sms * kStreamPairsPerSm;
             if (!alloc_bytes((void**)&d_sk_partials, sizeof(float4) * 2 * kStreamTileVoxels * (size_t)pairs))
                 return false;
