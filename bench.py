@@ -706,6 +706,17 @@ def _event_ms(fn, reps, warmup):
     return a.elapsed_time(b) / reps
 
 
+_FP32 = []
+
+
+def calibrate_fp32_cached():
+    """The measured FP32 FMA rate (TFLOP/s), probed once per process."""
+    if not _FP32:
+        from cuda_ultrasound_toolkit_b200.api import calibrate_fp32
+        _FP32.append(calibrate_fp32())
+    return _FP32[0]
+
+
 def sequences_section(reps=5, warmup=3, seed=11):
     """The other live sequences and the bandpass input, each on the GPU with the FP64 oracle timed
     beside it on a bounded sample.
@@ -724,13 +735,17 @@ def sequences_section(reps=5, warmup=3, seed=11):
     rng = np.random.default_rng(seed)
     out = {}
     T, C, S, X, Z = 64, 128, 2048, 256, 512
-    for name in ("tpw", "uforces"):
+    # "tpw" / "uforces": the volume spans the whole aperture (x step 0.15 mm: the staged windows of a
+    # 32-voxel-wide tile overflow, so the default engine is one thread per voxel); "_fine": a 9.6 mm
+    # wide volume (x step 0.038 mm), on the staged engine
+    for name in ("tpw", "uforces", "tpw_fine", "uforces_fine"):
+        half = (C * synth.PITCH / 2) if not name.endswith("_fine") else 4.8e-3
         w = synth.Workload(name, T, C, S, X, 1, Z, 0, cubic=True, cf=1.0)
         bp = synth.make_params(w)
         bp.tx_orientation = bp.rx_orientation  # x-z plane
-        bp.output_min_coordinate[0], bp.output_max_coordinate[0] = -C * synth.PITCH / 2, C * synth.PITCH / 2
+        bp.output_min_coordinate[0], bp.output_max_coordinate[0] = -half, half
         bp.fn_rx = 1.0
-        if name == "tpw":
+        if name.startswith("tpw"):
             bp.das_shader_id = int(SequenceId.RCA_TPW)
             for t, ang in enumerate(np.linspace(-0.25, 0.25, T)):
                 bp.foci[3 * t + 2] = float(ang)
@@ -746,6 +761,10 @@ def sequences_section(reps=5, warmup=3, seed=11):
         vol = plan.empty_volume()
         ms = _event_ms(lambda: plan.das(iq, out=vol), reps, warmup)
         plan.check()
+        direct = Plan(bp, das_tile=3)  # the one-thread-per-voxel kernel, for comparison
+        vol_d = direct.empty_volume()
+        direct_ms = _event_ms(lambda: direct.das(iq, out=vol_d), reps, warmup)
+        direct.check()
         vtc = X * Z * used * C
         n_vox = 256
         vox = rng.choice(X * Z, n_vox, replace=False)
@@ -754,8 +773,12 @@ def sequences_section(reps=5, warmup=3, seed=11):
         ref = O.das(iq_h, bp, vox, threads)
         cpu_s = time.perf_counter() - t0
         got = vol.cpu().numpy().reshape(-1)[vox]
-        out[name] = {"workload": f"{T} tx x {C} ch x {S} samples -> {X} x 1 x {Z}, cubic + CF",
-                     "device_ms": ms, "vtc_per_s": vtc / ms * 1e3,
+        engine = "one thread per voxel (das_direct.cu)" if plan.tile_shape == (1, 1, 1) else "staged windows (das.cu)"
+        out[name] = {"workload": f"{T} tx x {C} ch x {S} samples -> {X} x 1 x {Z} over x in +-{half * 1e3:.1f} mm, "
+                                 "cubic + CF",
+                     "device_ms": ms, "vtc_per_s": vtc / ms * 1e3, "engine": engine,
+                     "one_thread_per_voxel_ms": direct_ms,
+                     "fp32_frac": vtc * 49 / (ms * 1e-3) / 1e12 / calibrate_fp32_cached(),
                      "rel_l2_vs_fp64_sample": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
                      "cpu_baseline": {"vtc_per_s": n_vox * used * C / cpu_s, "cores": threads, "kind": "port",
                                       "sample": f"FP64 oracle, {n_vox} random voxels"}}

@@ -553,7 +553,9 @@ __device__ __forceinline__ void row_pass(const DasArgs& a, const Smem<IQ, NCS, D
             if constexpr (Q::kTpw || Q::kUf) {
                 // receive Hann window; the windowed value enters both sums (beamformer_kernels.cu:93-172,
                 // 490-550). TPW skips windows below 0.1; UFORCES scales the first transmit by 1/sqrt(128).
-                apo = hann_apo(fabsf(rx), vzv[v], a.fn_rx);
+                // vzv holds fn_rx / (2 depth) here: one multiply instead of a division per voxel and row
+                const float c = __cosf(kPi * fminf(fabsf(rx) * vzv[v], 0.5f));
+                apo = c * c;
                 if (Q::kTpw && apo < 0.1f) continue;
                 apo *= st.uni_apo;
             } else if (HERC) {
@@ -800,6 +802,8 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
     for (int v = 0; v < kVpt; ++v) {
         dz[v] = ((float)(z_first + v) - iz_c) * a.res_z;
         vzv[v] = fmaf((float)(z_first + v), a.res_z, a.vmin_z);
+        // TPW / UFORCES: only the receive Hann window reads the depth, as fn_rx / (2 depth)
+        if constexpr (Seq<SEQ>::kTpw || Seq<SEQ>::kUf) vzv[v] = a.fn_rx * 0.5f / vzv[v];
         txs[v] = 0.f;
         if (HERC) {
             // Transmit path of this voxel relative to the centre's (FP64), in samples.
@@ -1174,23 +1178,24 @@ das_stream_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a
     }
 }
 
-// Split form for volumes of fewer tiles than half a wave (small 2-D slices of the y-invariant
-// sequences): CTA (blockIdx.x, blockIdx.y) sums stage slice blockIdx.y of gridDim.y of tile
-// blockIdx.x (id order: z-major, then y, then x), and the last slice to finish a tile adds all
-// slices (the kPartSplit protocol of das_tile, through a.sk_partials / a.sk_counters).
+// Split form: CTA (blockIdx.x, blockIdx.y) sums stage slice blockIdx.y of gridDim.y of tile
+// tile_base + blockIdx.x (id order: z-major, then y, then x), and the last slice to finish a tile
+// adds all slices (the kPartSplit protocol of das_tile; records and counters indexed by blockIdx.x
+// in a.sk_partials / a.sk_counters). With one slice it is the grid kernel over a range of tile ids.
+// Used for volumes of fewer tiles than half a wave, and for the partial last wave of larger ones.
 template <int SEQ, bool CUBIC, bool CF, bool APO, class IQ, bool SHORT, bool DB>
 __global__ void __launch_bounds__(kThreads, 3)
-das_split_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
+das_split_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a, int tile_base)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     auto& sm = *reinterpret_cast<Smem<IQ, coef_arrays<SEQ, CUBIC, APO>(), DB>*>(smem_raw);
     using L = Layout<SEQ, SHORT>;
     const int nx = div_up(a.X, L::TX), ny = Seq<SEQ>::k3d ? div_up(a.Y, L::TY) : 1;
-    const int tile = blockIdx.x, P = gridDim.y, p = blockIdx.y;
+    const int tile = tile_base + (int)blockIdx.x, P = gridDim.y, p = blockIdx.y;
     const long long nst = tile_stages(a);
     das_tile<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>(iq, vol, a, sm, tile % nx, (tile / nx) % ny, tile / (nx * ny),
-                                                 (int)(nst * p / P), (int)(nst * (p + 1) / P), kPartSplit, p, P,
-                                                 tile);
+                                                 (int)(nst * p / P), (int)(nst * (p + 1) / P),
+                                                 P > 1 ? kPartSplit : kPartFull, p, P, (int)blockIdx.x);
 }
 
 // Persistent delay-and-sum over the tiles of many frames: CTAs take (frame, tile) work items,
@@ -1251,23 +1256,31 @@ bool launch_das_k(const DasArgs& a, const void* iq, void* volume, cudaStream_t s
     CUTB_REQUIRE(grid.y <= 65535 && grid.z <= 65535, CUTB_ERR_UNSUPPORTED, "Output grid too large.");
     auto kern = das_kernel<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>;
     const size_t smem = sizeof(Smem<IQ, coef_arrays<SEQ, CUBIC, APO>(), DB>);
-    if (!a.tiles && a.sk_partials && a.sk_counters && SEQ != HERCULES) {
-        // Fewer tiles than half a wave: split every tile's stages over P CTAs (at least 8 stages
-        // each) so that the volume still fills the GPU.
+    if (!a.tiles && a.sk_partials && a.sk_counters && a.schedule != 2 && a.schedule != 1) {
+        // Split every tile of a small volume (fewer tiles than half a wave; not HERCULES, whose
+        // small frames the batched kernel runs whole), or the tiles of a partial last wave of a
+        // large one, over P CTAs of at least kBatch stages each, so that the GPU stays full.
         auto pkern = das_split_kernel<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>;
         static std::atomic<uint64_t> sp_smem_set{0};
         static std::atomic<int> sp_wave[64];
         if (!set_smem_limit(pkern, smem, sp_smem_set)) return false;
         int wave = 0;
         if (!wave_size(pkern, smem, sp_wave, &wave)) return false;
-        const long long tiles = (long long)grid.x * grid.y * grid.z;
-        const long long P = std::min<long long>(std::min<long long>(wave / std::max<long long>(tiles, 1),
-                                                                    tile_stages(a) / kBatch),
-                                                2LL * a.sk_capacity / std::max<long long>(tiles, 1));
         if (g_prepare_only) return true;
-        if (2 * tiles <= wave && P >= 2 && tiles <= a.sk_capacity) {
-            CUTB_CUDA_OK(cudaMemsetAsync(a.sk_counters, 0, sizeof(int) * (size_t)tiles, st));
-            pkern<<<dim3((unsigned)tiles, (unsigned)P), kThreads, smem, st>>>((const IQ*)iq, (float2*)volume, a);
+        const long long tiles = (long long)grid.x * grid.y * grid.z;
+        const long long tail = tiles > wave ? tiles % wave : (SEQ != HERCULES ? tiles : 0);
+        const long long P = tail > 0 ? std::min<long long>(std::min<long long>(wave / tail, tile_stages(a) / kBatch),
+                                                           2LL * a.sk_capacity / tail)
+                                     : 0;
+        if (tail > 0 && 2 * tail <= wave && P >= 2 && tail <= a.sk_capacity) {
+            const long long whole = tiles - tail;
+            if (whole > 0) {
+                pkern<<<dim3((unsigned)whole, 1), kThreads, smem, st>>>((const IQ*)iq, (float2*)volume, a, 0);
+                CUTB_CUDA_OK(cudaGetLastError());
+            }
+            CUTB_CUDA_OK(cudaMemsetAsync(a.sk_counters, 0, sizeof(int) * (size_t)tail, st));
+            pkern<<<dim3((unsigned)tail, (unsigned)P), kThreads, smem, st>>>((const IQ*)iq, (float2*)volume, a,
+                                                                             (int)whole);
             CUTB_CUDA_OK(cudaGetLastError());
             return true;
         }
@@ -1488,12 +1501,36 @@ bool derive_das(const CudaBeamformerParameters& bp, DasArgs& a)
 
 // Sequences whose voxels differ in y within a tile: HERCULES, and tilted plane waves in a y-z plane.
 static bool das_3d(const DasArgs& a) { return a.seq == HERCULES || (a.seq == RCA_TPW && a.focus == 2); }
-// TPW and UFORCES on the one-thread-per-voxel kernel (das_direct.cu) instead of the staged engine.
-static bool das_direct(const DasArgs& a) { return (a.seq == RCA_TPW || a.seq == UFORCES) && a.tile == 3; }
-
 static bool use_short_tile(const DasArgs& a)
 {
     return das_3d(a) && (a.tile == 2 || (a.tile == 0 && prefer_short_tile(a)));
+}
+
+// True when the staged windows of a TPW / UFORCES tile fit the stage buffers: the receive and the
+// transmit path each move the index by at most the tile radius times spm, and a window spans twice
+// that plus the interpolation taps. On coarse grids (wide tiles) the rows would be read from global
+// memory instead, where the one-thread-per-voxel kernel is faster.
+static bool seq_windows_fit(const DasArgs& a)
+{
+    double hx, hy = 0.0, hz;
+    if (das_3d(a)) {
+        const bool sh = use_short_tile(a);
+        hx = 0.5 * ((sh ? Layout<kTpwYz, true>::TX : Layout<kTpwYz, false>::TX) - 1) * std::fabs((double)a.res_x);
+        hy = 0.5 * (Layout<kTpwYz, false>::TY - 1) * std::fabs((double)a.res_y);
+        hz = 0.5 * ((sh ? Layout<kTpwYz, true>::TZ : Layout<kTpwYz, false>::TZ) - 1) * std::fabs((double)a.res_z);
+    } else {
+        hx = 0.5 * (Layout<UFORCES, false>::TX - 1) * std::fabs((double)a.res_x);
+        hz = 0.5 * (Layout<UFORCES, false>::TZ - 1) * std::fabs((double)a.res_z);
+    }
+    const double reach = std::sqrt(hx * hx + hy * hy + hz * hz) * (double)a.spm;
+    return 4.0 * reach + 8.0 <= (double)(kWinMax - 8);
+}
+
+// TPW and UFORCES on the one-thread-per-voxel kernel (das_direct.cu) instead of the staged engine:
+// on request (tile 3), or by default when the staged windows would not fit.
+static bool das_direct(const DasArgs& a)
+{
+    return (a.seq == RCA_TPW || a.seq == UFORCES) && (a.tile == 3 || (a.tile == 0 && !seq_windows_fit(a)));
 }
 
 bool das_staged(const DasArgs& a)
@@ -1565,6 +1602,10 @@ void das_grid_tiles(const DasArgs& a, int counts[3])
 
 void das_tile_shape(const DasArgs& a, int shape[3])
 {
+    if (das_direct(a)) {  // one thread per voxel: no tiles
+        shape[0] = shape[1] = shape[2] = 1;
+        return;
+    }
     const bool sh = use_short_tile(a);
     shape[0] = das_3d(a) ? (sh ? Layout<HERCULES, true>::TX : Layout<HERCULES, false>::TX) : Layout<FORCES, false>::TX;
     shape[1] = das_3d(a) ? 8 : 1;

@@ -103,7 +103,7 @@ struct DasArgs {
     double fc_fs;              // the same ratio formed in FP64 from the FP32 frequencies
     int tile;                  // 0 chosen from the grid, 1 = 4 x 8 x 32, 2 = 8 x 8 x 16 (HERCULES, TPW in a
                                // y-z plane), 3 = one thread per voxel (TPW, UFORCES)
-    int schedule;              // 0, 1: one CTA per tile; 2: stream-K beyond one wave
+    int schedule;              // 0: split partial last wave / small 2-D volumes, 1: one CTA per tile, 2: stream-K
     const int* tiles;          // optional device list of tile ids (z-major); null = every tile
     int ntiles;
     int splits;                // > 1: stages split across CTAs, partial sums added atomically

@@ -63,13 +63,15 @@ typedef struct cutb_options {
     int iq_bf16;      /* 1: analytic signal stored as bf16 complex (halves DAS gather bytes) */
     int das_tile;     /* delay-and-sum tile: 0 = chosen from the grid, 1 = 4x8x32, 2 = 8x8x16 (HERCULES and
                          TPW in a y-z plane), 3 = one thread per voxel instead of the staged engine
-                         (TPW and UFORCES only) */
+                         (TPW and UFORCES only; 0 also picks it when the staged windows of a coarse
+                         grid would not fit the stage buffers) */
     int decode_tc;    /* 1: int16 decode on int8 tensor cores (hi/lo byte split, exact); needs 32..256
                          transmits in steps of 32 and rows of 8-sample multiples */
-    int das_schedule; /* delay-and-sum schedule: 0 = default (one CTA per tile), 1 = one CTA per tile,
-                         2 = stream-K when the tiles exceed one wave: the last waves' tiles x stages
-                         split evenly over the resident CTAs, partial sums combined through plan-owned
-                         scratch memory */
+    int das_schedule; /* delay-and-sum schedule: 0 = default: one CTA per tile, except that the tiles
+                         of a partial last wave (and every tile of a small TPW / UFORCES / FORCES
+                         volume) are split over several CTAs whose partial sums meet in plan-owned
+                         scratch memory; 1 = one CTA per tile; 2 = stream-K when the tiles exceed one
+                         wave (the last waves' tiles x stages split evenly over the resident CTAs) */
     int reserved[12];
 } cutb_options;
 
@@ -98,17 +100,16 @@ CUTB_API bool cutb_decode(cutb_plan* plan, const void* d_raw, size_t raw_bytes, 
  * CUTB_ERR_UNSUPPORTED. */
 CUTB_API bool cutb_hilbert(cutb_plan* plan, const float* d_in, uint in_stride, void* d_iq, void* stream);
 
-/* Delay-and-sum of d_iq [T][C][S] into the complex64 volume d_volume [Z][Y][X]. With
- * das_schedule = 2 a volume of more than one wave of tiles (SMs x resident CTAs) is split stream-K
- * style and the two CTAs that share a tile combine their sums through scratch memory the plan
- * owns; calls of one plan must then not overlap on the GPU. */
+/* Delay-and-sum of d_iq [T][C][S] into the complex64 volume d_volume [Z][Y][X]. Tiles may be split
+ * over several CTAs that combine their partial sums through scratch memory the plan owns (see
+ * cutb_options.das_schedule), so calls of one plan must not overlap on the GPU. */
 CUTB_API bool cutb_das(cutb_plan* plan, const void* d_iq, void* d_volume, void* stream);
 
 /* Whole pipeline on device memory, intermediates in the plan's own buffers. */
 CUTB_API bool cutb_beamform(cutb_plan* plan, const void* d_raw, size_t raw_bytes, void* d_volume, void* stream);
 
 /* Tile shape (x, y, z voxels) of this plan's delay-and-sum; tile id = (tz * ny + ty) * nx + tx
- * with nx = ceil(X / shape[0]) etc. */
+ * with nx = ceil(X / shape[0]) etc. (1, 1, 1) for the one-thread-per-voxel kernel. */
 CUTB_API bool cutb_plan_das_tile_shape(const cutb_plan* plan, uint shape[3]);
 
 /* Delay-and-sum of the listed tiles only (host array of tile ids), each tile's transmit x channel
@@ -152,7 +153,8 @@ CUTB_API bool cutb_plan_check(cutb_plan* plan, void* stream);
  * 0.2 s), the CTA stops, waits for the copies it had already issued and leaves; cutb_plan_check
  * then reports CUTB_ERR_TIMEOUT. stage = -1 turns the hook off. The volume of such a call is
  * undefined. No GPU fault is involved: every wait stays bounded. Every sequence runs on the staged
- * engine except TPW / UFORCES plans created with das_tile = 3, which are rejected here. */
+ * engine except TPW / UFORCES plans on the one-thread-per-voxel kernel (das_tile = 3, or 0 on a grid
+ * too coarse for the staged windows), which are rejected here. */
 CUTB_API bool cutb_debug_das_skip_stage(cutb_plan* plan, int stage, long long wait_limit_cycles);
 
 /* Number of kernels the last cutb_beamform/cutb_decode/cutb_hilbert/cutb_das call launched. */

@@ -57,7 +57,7 @@ def params(kind):
 # raw taps, no coefficients; forces: the y-invariant sequence; tpw_xz / tpw_yz: tilted plane waves
 # (y-invariant, and over y); uforces: sparse transmit elements after a flash.
 CASES = [("default", 0), ("long", 1), ("apo", 0), ("linear", 0), ("linear_apo", 0), ("forces", 0),
-         ("tpw_xz", 0), ("tpw_yz", 0), ("uforces", 0)]
+         ("tpw_xz", 2), ("tpw_yz", 2), ("uforces", 2)]  # tile 2: the staged engine on this coarse grid
 
 
 @pytest.mark.parametrize("kind,tile", CASES)

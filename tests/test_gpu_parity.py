@@ -143,7 +143,7 @@ def test_hilbert_strided_input_and_known_answer(torch, orc):
 # ---------------------------------------------------------------------------------------------
 def das_params(seq=SequenceId.HERCULES, cubic=True, cf=0.0, fn_rx=0.0, fn_tx=0.0, apo=ApoType.RX_HANN,
                readi=0, readi_id=0, decode=EncodingMatrix.HADAMARD, focus_z=math.inf, S=512, C=8, T=8,
-               X=20, Y=9, Z=40, z=(4e-3, 26e-3), time_offset=0.0):
+               X=20, Y=9, Z=40, z=(4e-3, 26e-3), time_offset=0.0, x=(-3e-3, 3e-3)):
     bp = base_params(S, C, T, X=X, Y=Y, Z=Z, decode=decode)
     bp.das_shader_id = int(seq)
     bp.interpolate = bool(cubic)
@@ -153,7 +153,7 @@ def das_params(seq=SequenceId.HERCULES, cubic=True, cf=0.0, fn_rx=0.0, fn_tx=0.0
     bp.to_power = 2
     bp.readi_group_count, bp.readi_group_id = readi, readi_id
     bp.foci[2] = focus_z
-    bp.output_min_coordinate[0], bp.output_max_coordinate[0] = -3e-3, 3e-3
+    bp.output_min_coordinate[0], bp.output_max_coordinate[0] = x
     bp.output_min_coordinate[1] = -1e-3
     bp.output_min_coordinate[2], bp.output_max_coordinate[2] = z
     bp.time_offset = time_offset
@@ -274,13 +274,23 @@ TPW_UFORCES_CASES = [
     dict(seq=SequenceId.UFORCES, elems=[0, 2, 3, 5, 6, 8, 9, 11], same=True, focus_z=20e-3, fn_rx=1.0, cf=0.5),
     dict(seq=SequenceId.UFORCES, elems=list(range(8)), same=True, focus_z=30e-3, cf=1.0, cubic=False),
     dict(seq=SequenceId.UFORCES, elems=list(range(8)), same=True, focus_z=30e-3, cf=0.3, z=(0.0, 30e-3)),  # clamp at 0
+    # fine grids: the staged windows fit, so tile 0 takes the staged engine
+    dict(seq=SequenceId.RCA_TPW, angles=np.linspace(-0.2, 0.2, 8), same=True, cf=1.0, fn_rx=1.0, X=64, Z=64,
+         x=(-1.5e-3, 1.5e-3), z=(4e-3, 7e-3)),
+    dict(seq=SequenceId.RCA_TPW, angles=np.linspace(-0.2, 0.2, 8), cf=0.5, X=32, Y=16, Z=48,
+         x=(-0.8e-3, 0.8e-3), z=(4e-3, 6e-3)),
+    dict(seq=SequenceId.UFORCES, elems=[0, 2, 3, 5, 6, 8, 9, 11], same=True, focus_z=20e-3, fn_rx=1.0, cf=0.5,
+         X=64, Z=64, x=(-1.5e-3, 1.5e-3), z=(4e-3, 7e-3)),
 ]
 
 
 @pytest.mark.parametrize("case", TPW_UFORCES_CASES, ids=lambda c: f"{int(c['seq'])}-" + "-".join(
     f"{k}" for k in c if k != "seq"))
 @pytest.mark.parametrize("bf16", [False, True])
-@pytest.mark.parametrize("tile", [0, 1, 3])  # staged engine (chosen / 4 x 8 x 32 tile), one thread per voxel
+# 0: chosen (one thread per voxel here, the grids are too coarse for the stage buffers); 1, 2: the staged
+# engine (TPW over y: 4 x 8 x 32 and 8 x 8 x 16 tiles; rows whose window overflows read global memory);
+# 3: one thread per voxel
+@pytest.mark.parametrize("tile", [0, 1, 2, 3])
 def test_das_tpw_uforces_vs_fp64(torch, orc, case, bf16, tile):
     case = dict(case)
     angles, elems, same = case.pop("angles", None), case.pop("elems", None), case.pop("same", False)
