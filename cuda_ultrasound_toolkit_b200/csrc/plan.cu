@@ -496,9 +496,9 @@ bool cutb_plan::build(const CudaBeamformerParameters& params, const cutb_options
         CUTB_CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         das_grid_tiles(das, counts);
         const long long tiles = (long long)counts[0] * counts[1] * counts[2];
-        // volumes beyond one wave (a split last wave, or stream-K), and small volumes of the
-        // sequences other than HERCULES (every tile split)
-        if (das.schedule != 1 && (tiles > sms || (das.seq != HERCULES && 2 * tiles <= 3LL * sms))) {
+        // stream-K beyond one wave (on request); the sequences other than HERCULES split a small
+        // volume's tiles or a partial last wave
+        if ((das.schedule == 2 && tiles > sms) || (das.schedule == 0 && das.seq != HERCULES)) {
             const int pairs = sms * kStreamPairsPerSm;
             if (!alloc_bytes((void**)&d_sk_partials, sizeof(float4) * 2 * kStreamTileVoxels * (size_t)pairs))
                 return false;

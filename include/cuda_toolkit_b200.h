@@ -67,11 +67,11 @@ typedef struct cutb_options {
                          grid would not fit the stage buffers) */
     int decode_tc;    /* 1: int16 decode on int8 tensor cores (hi/lo byte split, exact); needs 32..256
                          transmits in steps of 32 and rows of 8-sample multiples */
-    int das_schedule; /* delay-and-sum schedule: 0 = default: one CTA per tile, except that the tiles
-                         of a partial last wave (and every tile of a small TPW / UFORCES / FORCES
-                         volume) are split over several CTAs whose partial sums meet in plan-owned
-                         scratch memory; 1 = one CTA per tile; 2 = stream-K when the tiles exceed one
-                         wave (the last waves' tiles x stages split evenly over the resident CTAs) */
+    int das_schedule; /* delay-and-sum schedule: 0 = default: one CTA per tile, except that FORCES,
+                         TPW and UFORCES split the tiles of a small volume (or of a partial last
+                         wave) over several CTAs whose partial sums meet in plan-owned scratch
+                         memory; 1 = one CTA per tile; 2 = stream-K when the tiles exceed one wave
+                         (the last waves' tiles x stages split evenly over the resident CTAs) */
     int reserved[12];
 } cutb_options;
 
