@@ -124,6 +124,19 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "of fallback"
 
 
+def shared_roofline(vct, cubic, das_ms, sm_mhz, sms=148):
+    """Shared-memory roofline of the delay-and-sum: algorithmic coefficient bytes (32 B cubic / 16 B
+    linear per voxel-transmit-channel) over the SMs' shared data path (128 B per clock per SM) at
+    the median SM clock sampled during the timed region."""
+    if not sm_mhz:
+        return None
+    nbytes = vct * (32 if cubic else 16)
+    achieved = nbytes / (das_ms * 1e-3) / 1e12
+    peak = sms * 128 * sm_mhz * 1e6 / 1e12
+    return {"bytes_per_launch": nbytes, "achieved_tbs": achieved, "peak_tbs": peak, "frac": achieved / peak,
+            "unit": "TB/s", "peak_source": f"{sms} SMs x 128 B/clk x {sm_mhz:.0f} MHz (sampled SM clock)"}
+
+
 def profile_traffic(name):
     """DRAM bytes per launch recorded by ncu for a kernel (profiles/<name>.json), if committed."""
     path = os.path.join(ROOT, "profiles", f"{name}.json")
@@ -343,7 +356,11 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"bound": "fp32", "kernel": "das", "achieved": das_tflops, "peak": fp32_peak,
                      "unit": "TFLOP/s", "frac": das_tflops / fp32_peak, "traffic": profile_traffic("das_full"),
                      "algorithmic": f"{flops_per_vct} FLOP per voxel-transmit-channel x {vct} per launch",
-                     "peak_source": "measured FP32 FMA probe (cutb_calibrate_fp32) on this GPU"},
+                     "peak_source": "measured FP32 FMA probe (cutb_calibrate_fp32) on this GPU",
+                     # the data path the kernel saturates first: every voxel-transmit-channel reads
+                     # its interval's four complex cubic coefficients (32 B) from shared memory, and
+                     # an SM moves 128 B of shared data per clock
+                     "shared_memory": shared_roofline(vct, bp.interpolate, stage_ms["das"], clock.get("sm_mhz"))},
         "stages": {
             "decode": {"ms": stage_ms["decode"], "achieved_gbs": dec_bytes / (stage_ms["decode"] * 1e-3) / 1e9,
                        "peak_gbs": hbm, "frac": dec_bytes / (stage_ms["decode"] * 1e-3) / 1e9 / hbm,
