@@ -166,7 +166,7 @@ __device__ __forceinline__ float2 interp_global(const IQ* row, float idx, int k_
 }
 
 // Per-row stage metadata written by the issuing lane.
-struct alignas(16) RowMeta {  // 16-byte aligned: neighbouring fields load as one vector
+struct RowMeta {
     float base;     // sample index at the tile centre, relative to `lo`
     float d0;       // FP32 copy of the centre-to-receive-point distance
     float d0sq;     // its square
@@ -207,11 +207,8 @@ struct alignas(128) Smem {
     static constexpr int kWin = DB ? kWinShort : kWinMax;
     static constexpr int kCB = DB ? 2 : 1;
     IQ raw[kStages][kRows][kWin];
-    // Rows of wint intervals, packed: interval i (1 .. len - 3) of row q at q * wint + i - 1, the
-    // build's item number, so a warp's stores are contiguous (a row stride of kWin put the two rows a
-    // warp straddles on the same banks).
-    float4 coefA[NC >= 1 ? kCB : 1][NC >= 1 ? kRows * kWin : 1];
-    float4 coefB[NC == 2 ? kCB : 1][NC == 2 ? kRows * kWin : 1];
+    float4 coefA[NC >= 1 ? kCB : 1][NC >= 1 ? kRows : 1][NC >= 1 ? kWin : 1];
+    float4 coefB[NC == 2 ? kCB : 1][NC == 2 ? kRows : 1][NC == 2 ? kWin : 1];
     RowMeta rowc[NC >= 1 ? kCB : 1][NC >= 1 ? kRows : 1];  // metadata of the rows whose coefficients are built
     RowMeta row[kStages][kRows];
     StageMeta stage[kStages];
@@ -226,11 +223,6 @@ struct alignas(128) Smem {
     int tx_reach_bits;
     int part_last;  // stream-K: the pair counter's value before this part's arrival
 };
-
-// Three CTAs per SM (228 KiB of shared memory, 1 KiB reserved per CTA) for the forms the full
-// benchmark frame uses; two would halve the warps that hide the row pass's latency.
-static_assert(3 * (sizeof(Smem<float2, 2, true>) + 1024) <= 228 * 1024, "double-buffered cubic form: 3 CTAs/SM");
-static_assert(3 * (sizeof(Smem<float2, 2, false>) + 1024) <= 228 * 1024, "cubic form: 3 CTAs/SM");
 
 // Coefficient arrays staged per row: cubic always 2; linear 1 where the packed row pass runs
 // (HERCULES without apodization), else 0 (the taps are read from the raw windows).
@@ -507,7 +499,7 @@ __device__ __forceinline__ void build_coefficients(Smem<IQ, NC, DB>& sm, int b, 
         if constexpr (NC == 1) {
             // linear: value(t) = p0 + t (p1 - p0), the operations of the scalar staged pass
             const float2 p0 = to_f2(p[i]), p1 = to_f2(p[i + 1]);
-            sm.coefA[cb][e] = make_float4(p0.x, p0.y, p1.x - p0.x, p1.y - p0.y);
+            sm.coefA[cb][q][i] = make_float4(p0.x, p0.y, p1.x - p0.x, p1.y - p0.y);
         } else {
             const float2 pm1 = to_f2(p[i - 1]), p0 = to_f2(p[i]), p1 = to_f2(p[i + 1]), p2 = to_f2(p[i + 2]);
             float4 A, B;
@@ -527,8 +519,8 @@ __device__ __forceinline__ void build_coefficients(Smem<IQ, NC, DB>& sm, int b, 
                 A = make_float4(a0.x, a0.y, a1.x, a1.y);
                 B = make_float4(b0.x, b0.y, b1.x, b1.y);
             }
-            sm.coefA[cb][e] = A;
-            sm.coefB[cb][e] = B;
+            sm.coefA[cb][q][i] = A;
+            sm.coefB[cb][q][i] = B;
         }
     }
 }
@@ -537,7 +529,7 @@ __device__ __forceinline__ void build_coefficients(Smem<IQ, NC, DB>& sm, int b, 
 // for cubic, raw taps for linear); otherwise from the global row with guarded taps.
 template <int SEQ, bool CUBIC, bool CF, bool APO, bool STAGED, class IQ, int NCS, bool DB>
 __device__ __forceinline__ void row_pass(const DasArgs& a, const Smem<IQ, NCS, DB>& sm, const RowMeta* rows, int b,
-                                         int qi, int wint, const IQ* grow, const StageMeta& st, float dxe, const float (&sq)[kVpt],
+                                         int qi, const IQ* grow, const StageMeta& st, float dxe, const float (&sq)[kVpt],
                                          const float (&txs)[kVpt], const float (&vzv)[kVpt], float vx, float a2,
                                          float2 (&total)[kVpt], float (&inc)[kVpt], const float2* rot_tab = nullptr)
 {
@@ -591,7 +583,7 @@ __device__ __forceinline__ void row_pass(const DasArgs& a, const Smem<IQ, NCS, D
             const float t = idx - (f - kMagic);
             if constexpr (CUBIC) {
                 static_assert(!DB, "the scalar staged pass reads the single coefficient buffer");
-                const float4 A = sm.coefA[0][qi * wint + i - 1], B = sm.coefB[0][qi * wint + i - 1];
+                const float4 A = sm.coefA[0][qi][i], B = sm.coefB[0][qi][i];
                 val.x = fmaf(fmaf(fmaf(B.z, t, B.x), t, A.z), t, A.x);
                 val.y = fmaf(fmaf(fmaf(B.w, t, B.y), t, A.w), t, A.y);
             } else {
@@ -681,7 +673,7 @@ __device__ __forceinline__ float rsqrt_approx(float x)
 // so d0^2 - (-delta) = d0^2 + delta. Only the coherence energy is kept as (re^2, im^2) partial
 // sums, added at the end.
 template <bool CF, bool CLAMP, class IQ, int NC, bool DB>
-__device__ __forceinline__ void row_pass_packed(const Smem<IQ, NC, DB>& sm, int cb, const RowMeta* rows, int qi, int wint, float dxe,
+__device__ __forceinline__ void row_pass_packed(const Smem<IQ, NC, DB>& sm, int cb, const RowMeta* rows, int qi, float dxe,
                                                 float spm, f2x ww, const f2x (&sq2)[kVpt / 2],
                                                 const f2x (&txs2)[kVpt / 2], f2x (&tot2)[kVpt], f2x (&inc2)[kVpt])
 {
@@ -693,8 +685,8 @@ __device__ __forceinline__ void row_pass_packed(const Smem<IQ, NC, DB>& sm, int 
     const f2x base2 = pk(m.base, m.base), spm2 = pk(spm, spm), mhalf2 = pk(-0.5f, -0.5f);
     const f2x magic2 = pk(kMagic, kMagic);
     const float loc = m.loclamp, hic = m.hiclamp;
-    const float4* cA = &sm.coefA[cb][qi * wint] - 1;  // interval i at cA[i]
-    const float4* cB = &sm.coefB[NC == 2 ? cb : 0][NC == 2 ? qi * wint : 0] - 1;
+    const float4* cA = sm.coefA[cb][qi];
+    const float4* cB = sm.coefB[NC == 2 ? cb : 0][NC == 2 ? qi : 0];
 #pragma unroll
     for (int p = 0; p < kVpt / 2; ++p) {
         const f2x nd = sub2(nexdx2, sq2[p]);  // -delta
@@ -969,36 +961,36 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
             if (unclamped && st.nq == kRows) {
 #pragma unroll
                 for (int qi = 0; qi < kRows; ++qi)
-                    row_pass_packed<CF, false>(sm, cb, rows, qi, wint, dxe, a.spm, ww, sq2, txs2, tot2, inc2);
+                    row_pass_packed<CF, false>(sm, cb, rows, qi, dxe, a.spm, ww, sq2, txs2, tot2, inc2);
             } else if (unclamped) {
 #pragma unroll 4
                 for (int qi = 0; qi < st.nq; ++qi)
-                    row_pass_packed<CF, false>(sm, cb, rows, qi, wint, dxe, a.spm, ww, sq2, txs2, tot2, inc2);
+                    row_pass_packed<CF, false>(sm, cb, rows, qi, dxe, a.spm, ww, sq2, txs2, tot2, inc2);
             } else if (all_staged) {
 #pragma unroll 4
                 for (int qi = 0; qi < st.nq; ++qi)
-                    row_pass_packed<CF, true>(sm, cb, rows, qi, wint, dxe, a.spm, ww, sq2, txs2, tot2, inc2);
+                    row_pass_packed<CF, true>(sm, cb, rows, qi, dxe, a.spm, ww, sq2, txs2, tot2, inc2);
             } else {
                 for (int qi = 0; qi < st.nq; ++qi) {
                     if (rows[qi].len > 0)
-                        row_pass_packed<CF, true>(sm, cb, rows, qi, wint, dxe, a.spm, ww, sq2, txs2, tot2, inc2);
+                        row_pass_packed<CF, true>(sm, cb, rows, qi, dxe, a.spm, ww, sq2, txs2, tot2, inc2);
                     else
-                        row_pass<SEQ, CUBIC, CF, APO, false>(a, sm, rows, b, qi, wint, grow0 + (size_t)qi * a.S, st, dxe, sq,
+                        row_pass<SEQ, CUBIC, CF, APO, false>(a, sm, rows, b, qi, grow0 + (size_t)qi * a.S, st, dxe, sq,
                                                              tsh, vzv, vx, a2, total, inc);
                 }
             }
         } else if (all_staged) {
 #pragma unroll 2
             for (int qi = 0; qi < st.nq; ++qi)
-                row_pass<SEQ, CUBIC, CF, APO, true>(a, sm, rows, b, qi, wint, grow0, st, dxe, sq, tsh, vzv, vx, a2, total,
+                row_pass<SEQ, CUBIC, CF, APO, true>(a, sm, rows, b, qi, grow0, st, dxe, sq, tsh, vzv, vx, a2, total,
                                                     inc, rot_tab);
         } else {
             for (int qi = 0; qi < st.nq; ++qi) {
                 if (rows[qi].len > 0)
-                    row_pass<SEQ, CUBIC, CF, APO, true>(a, sm, rows, b, qi, wint, grow0, st, dxe, sq, tsh, vzv, vx, a2, total,
+                    row_pass<SEQ, CUBIC, CF, APO, true>(a, sm, rows, b, qi, grow0, st, dxe, sq, tsh, vzv, vx, a2, total,
                                                         inc, rot_tab);
                 else
-                    row_pass<SEQ, CUBIC, CF, APO, false>(a, sm, rows, b, qi, wint, grow0 + (size_t)qi * a.S, st, dxe, sq, tsh,
+                    row_pass<SEQ, CUBIC, CF, APO, false>(a, sm, rows, b, qi, grow0 + (size_t)qi * a.S, st, dxe, sq, tsh,
                                                          vzv, vx, a2, total, inc, rot_tab);
             }
         }
