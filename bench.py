@@ -215,12 +215,12 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
-def upstream_gpu_section(raw, bp, ours_vol, reps=3):
+def upstream_gpu_section(raw, bp, ours_vol, reps=3, fp64=None):
     """Upstream's own CUDA build (baseline/_ref, built by baseline/Makefile for sm_100a) timed
     through its cuda_toolkit::beamform on host buffers, in a child process, on the benchmark
     frame with the settings upstream honours: cubic interpolation and no coherence factor
     (upstream's HERCULES kernel computes the factor but never applies it). `ours_vol` is this
-    library's volume of the same frame and settings."""
+    library's volume of the same frame and settings; fp64 = (voxels, FP64 oracle volume there)."""
     import subprocess
     import tempfile
     lib = os.path.join(ROOT, "baseline", "_ref", "libcuda_toolkit_upstream.so")
@@ -239,6 +239,10 @@ def upstream_gpu_section(raw, bp, ours_vol, reps=3):
         if os.path.exists(os.path.join(d, "volume.npy")):
             ref = np.load(os.path.join(d, "volume.npy"))
             out["rel_l2_ours_vs_upstream"] = float(np.linalg.norm(ours_vol - ref) / np.linalg.norm(ref))
+            if fp64 is not None:
+                vox, exact = fp64
+                rel = lambda v: float(np.linalg.norm(v.reshape(-1)[vox] - exact) / np.linalg.norm(exact))  # noqa: E731
+                out["rel_l2_vs_fp64"] = {"upstream": rel(ref), "ours": rel(ours_vol), "voxels": len(vox)}
     out["settings"] = "interpolate=true (cubic), coherency_weighting=0; same frame"
     return out
 
@@ -413,18 +417,23 @@ def run_ours(args, rank, world, local_rank):
         line["parity"] = full_frame_parity(plans[0], d_raw[0], frames[0][0], bp, iq_ref, threads)
     except Exception as exc:  # must not hide the plain pipeline's number
         line["parity"] = {"failed": str(exc)}
-    del iq_ref
     if args.upstream and world == 1:
         try:
             ref_bp = bp.copy()
             ref_bp.coherency_weighting = 0.0
+            fp64 = None
+            if iq_ref is not None:  # FP64 volume of upstream's settings on the parity voxels
+                from oracle import oracle as O
+                z, y, x = bp.volume_shape
+                vox = np.sort(np.random.default_rng(21).choice(x * y * z, PARITY_VOXELS, replace=False))
+                fp64 = (vox, O.das(iq_ref, ref_bp, vox, threads))
             ours = beamform(frames[0][0], ref_bp)
             e2e_ref = []
             for _ in range(3):
                 t = time.perf_counter()
                 beamform(frames[0][0], ref_bp, out=ours)
                 e2e_ref.append(time.perf_counter() - t)
-            up = upstream_gpu_section(frames[0][0], ref_bp, ours)
+            up = upstream_gpu_section(frames[0][0], ref_bp, ours, fp64=fp64)
             up["ours_same_settings"] = {"ms": 1e3 * float(np.median(e2e_ref)),
                                         "volumes_per_s": 1.0 / float(np.median(e2e_ref)),
                                         "api": "cuda_toolkit::beamform (host spans)"}
@@ -433,6 +442,7 @@ def run_ours(args, rank, world, local_rank):
             line["upstream_gpu"] = up
         except Exception as exc:  # must not hide the plain pipeline's number
             line["upstream_gpu"] = {"failed": str(exc)}
+    del iq_ref
     print(json.dumps(line), flush=True)
 
 

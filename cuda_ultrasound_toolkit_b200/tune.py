@@ -1,7 +1,9 @@
-"""Autotuner for the delay-and-sum tile shape.
+"""Autotuner for the delay-and-sum tile shape and engine.
 
-For a parameter block it times the delay-and-sum of every candidate tile shape (the 4 x 8 x 32
-and 8 x 8 x 16 HERCULES tiles) on the device with CUDA events and keeps the fastest. Results
+For a parameter block it times the delay-and-sum of every candidate (`candidates`) on the device
+with CUDA events and keeps the fastest: the 4 x 8 x 32 and 8 x 8 x 16 tiles for HERCULES and for
+tilted plane waves in a y-z plane, and, for TPW and UFORCES, the staged engine against the
+one-thread-per-voxel kernel (which wins on grids too coarse for the staged windows). Results
 are keyed by everything that changes the kernel's work per tile -- dimensions, grid steps,
 interpolation, coherence factor, apodization, storage -- and kept in memory and, when a cache
 path is given, in a JSON file that later runs reload.
@@ -13,7 +15,20 @@ import torch
 
 from .api import Plan
 
-CANDIDATES = (1, 2)
+CANDIDATES = (1, 2)  # HERCULES: 4 x 8 x 32, 8 x 8 x 16
+
+
+def candidates(bp):
+    """das_tile values worth timing for this parameter block (cutb_options.das_tile)."""
+    from .params import SequenceId
+    seq = int(bp.das_shader_id)
+    if seq == SequenceId.HERCULES:
+        return CANDIDATES
+    if seq == SequenceId.RCA_TPW and bp.tx_orientation != bp.rx_orientation:  # plane waves over y
+        return (1, 2, 3)
+    if seq in (SequenceId.RCA_TPW, SequenceId.UFORCES):
+        return (2, 3)  # the staged engine (y-invariant layout), one thread per voxel
+    return (0,)
 
 
 def key(bp, iq_bf16=False):
@@ -57,7 +72,7 @@ class DasTuner:
         """The fastest tile id for this parameter block (measured once per key)."""
         k = key(bp)
         if k not in self.table:
-            ms = {str(t): self.measure(bp, t, iq) for t in CANDIDATES}
+            ms = {str(t): self.measure(bp, t, iq) for t in candidates(bp)}
             best = min(ms, key=ms.get)
             self.table[k] = {"tile": int(best), "ms": ms}
             self.save()

@@ -9,7 +9,7 @@ import pytest
 import torch
 
 from cuda_ultrasound_toolkit_b200 import Batch, Plan, batched
-from cuda_ultrasound_toolkit_b200.tune import DasTuner, CANDIDATES
+from cuda_ultrasound_toolkit_b200.tune import DasTuner, CANDIDATES, candidates
 
 pytestmark = pytest.mark.gpu
 
@@ -104,3 +104,23 @@ def test_tuner_choice_is_fastest_on_remeasure(tmp_path):
     # persisted and reloaded without measuring again
     again = DasTuner(str(tmp_path / "tiles.json"))
     assert again.choose(bp) == best
+
+
+@pytest.mark.parametrize("half", [19.2e-3, 2.4e-3])  # a coarse grid over the aperture, a fine one
+def test_tuner_picks_the_engine_for_tpw(tmp_path, half):
+    """For tilted plane waves the tuner times the staged engine against one thread per voxel."""
+    import numpy as np
+    from cuda_ultrasound_toolkit_b200 import SequenceId, synth
+    w = synth.Workload("tpw", 32, 64, 1024, 128, 1, 128, 0, cubic=True, cf=1.0, z_range=(5e-3, 20e-3))
+    bp = synth.make_params(w)
+    bp.das_shader_id = int(SequenceId.RCA_TPW)
+    bp.tx_orientation = bp.rx_orientation
+    bp.output_min_coordinate[0], bp.output_max_coordinate[0] = -half, half
+    bp.fn_rx = 1.0
+    for t, a in enumerate(np.linspace(-0.2, 0.2, 32)):
+        bp.foci[3 * t + 2] = float(a)
+    tuner = DasTuner(str(tmp_path / "tiles.json"), reps=3)
+    best = tuner.choose(bp)
+    assert best in candidates(bp) == (2, 3)
+    times = {t: tuner.measure(bp, t, reps=5) for t in candidates(bp)}
+    assert times[best] <= 1.15 * min(times.values()), times
