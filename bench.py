@@ -331,8 +331,31 @@ def run_ours(args, rank, world, local_rank):
     e2e_s = time.perf_counter() - t0
     barrier()
 
+    # One frame split over the ranks by z-slabs (broadcast of the raw frame, every rank's slab,
+    # all-gather of the slabs): the latency of a single frame on N GPUs. Every rank takes part.
+    sharded_ms = None
+    if world > 1:
+        from cuda_ultrasound_toolkit_b200.sharded import ShardedFrame
+        sf = ShardedFrame(bp, rank, world)
+        d_frame = d_raw[0].clone()
+        sf.beamform(d_frame)
+        torch.cuda.synchronize()
+        barrier()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(3):
+            sf.beamform(d_frame)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        sf.plan.check()
+        sharded_ms = s0.elapsed_time(s1) / 3
+        del sf, d_frame
+
     # Max over ranks.
     ms, e2e_s = max_over_ranks([ms, e2e_s], world, dev)
+    if sharded_ms is not None:
+        sharded_ms = max_over_ranks([sharded_ms], world, dev)[0]
     if rank != 0:
         return
 
@@ -377,6 +400,11 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": launches,
         "clocks": clock,
     }
+    if sharded_ms is not None:
+        line["single_frame_zslabs"] = {
+            "ms_per_frame": sharded_ms, "volumes_per_s": 1e3 / sharded_ms, "ranks": world,
+            "what": "one frame split by voxel z-slabs: NCCL broadcast of the raw frame, decode + Hilbert on "
+                    "every rank, each rank's slab (cutb_das_zslab), all-gather of the slabs; max over ranks"}
     if args.learned > 0 and world == 1:
         line["learned"] = learned_path(args.learned)
     if args.precision and world == 1:

@@ -79,6 +79,7 @@ def lib():
         "cutb_batch_launches_per_run": ([vp], ctypes.c_int),
         "cutb_batch_das_launches": ([vp], ctypes.c_int),
         "cutb_das_tiles": ([vp, vp, vp, ctypes.POINTER(ctypes.c_int), u, u, vp], b),
+        "cutb_das_zslab": ([vp, vp, vp, u, u, vp], b),
         "init_cuda_configuration": ([ctypes.POINTER(u), ctypes.POINTER(u)], b),
         "register_cuda_buffers": ([ctypes.POINTER(u), u, u], b),
         "cuda_set_channel_mapping": ([ctypes.POINTER(ctypes.c_int16)], b),
@@ -356,6 +357,16 @@ class Plan:
         shape = (ctypes.c_uint * 3)()
         _check(lib().cutb_plan_das_tile_shape(self._h, shape), "cutb_plan_das_tile_shape")
         return tuple(shape)
+
+    def das_zslab(self, iq, z0, z1, out=None, stream=None):
+        """Delay-and-sum of the z-planes z0 .. z1 - 1 into a [z1 - z0][Y][X] slab (cutb_das_zslab)."""
+        import torch
+        z, y, x = self.bp.volume_shape
+        if out is None:
+            out = torch.empty((z1 - z0, y, x), dtype=torch.complex64, device="cuda")
+        _check(lib().cutb_das_zslab(self._h, iq.data_ptr(), out.data_ptr(), int(z0), int(z1), _stream_handle(stream)),
+               "cutb_das_zslab")
+        return out
 
     def das_tiles(self, iq, tiles, splits=1, out=None, stream=None):
         """Delay-and-sum of the listed tile ids only (others zero), stages split over `splits` CTAs."""

@@ -1089,13 +1089,13 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
             out.y *= cf;
         }
         if (a.splits > 1) {  // partial sums over a slice of the stages (no coherence factor)
-            float2* o = vol + ((size_t)z * a.Y + y_idx) * a.X + x_idx;
+            float2* o = vol + ((size_t)(z - a.z_out0) * a.Y + y_idx) * a.X + x_idx;
             atomicAdd(&o->x, out.x);
             atomicAdd(&o->y, out.y);
         } else if (Y3) {
-            vol[((size_t)z * a.Y + y_idx) * a.X + x_idx] = out;
+            vol[((size_t)(z - a.z_out0) * a.Y + y_idx) * a.X + x_idx] = out;
         } else {  // y-invariant: one value for every y
-            for (int y = 0; y < a.Y; ++y) vol[((size_t)z * a.Y + y) * a.X + x_idx] = out;
+            for (int y = 0; y < a.Y; ++y) vol[((size_t)(z - a.z_out0) * a.Y + y) * a.X + x_idx] = out;
         }
     }
 }
@@ -1109,7 +1109,7 @@ das_kernel(const IQ* __restrict__ iq, float2* __restrict__ vol, DasArgs a)
     extern __shared__ __align__(128) unsigned char smem_raw[];
     auto& sm = *reinterpret_cast<Smem<IQ, coef_arrays<SEQ, CUBIC, APO>(), DB>*>(smem_raw);
     using L = Layout<SEQ, SHORT>;
-    int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
+    int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z + a.z_tile0;
     const int nst = tile_stages(a);
     int k_lo = 0, k_hi = nst;
     if (a.tiles) {
@@ -1251,12 +1251,13 @@ bool launch_das_k(const DasArgs& a, const void* iq, void* volume, cudaStream_t s
 {
     using L = Layout<SEQ, SHORT>;
     // FORCES does not depend on y: one y-slice of tiles, each written to every y.
-    dim3 grid(div_up(a.X, L::TX), Seq<SEQ>::k3d ? div_up(a.Y, L::TY) : 1, div_up(a.Z, L::TZ));
+    dim3 grid(div_up(a.X, L::TX), Seq<SEQ>::k3d ? div_up(a.Y, L::TY) : 1,
+              a.z_tiles > 0 ? a.z_tiles : div_up(a.Z, L::TZ));  // a z-slab: tiles z_tile0 .. + z_tiles - 1
     if (a.tiles) grid = dim3(a.ntiles, a.splits > 1 ? a.splits : 1, 1);
     CUTB_REQUIRE(grid.y <= 65535 && grid.z <= 65535, CUTB_ERR_UNSUPPORTED, "Output grid too large.");
     auto kern = das_kernel<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>;
     const size_t smem = sizeof(Smem<IQ, coef_arrays<SEQ, CUBIC, APO>(), DB>);
-    if (!a.tiles && a.sk_partials && a.sk_counters && a.schedule != 2 && a.schedule != 1) {
+    if (!a.tiles && a.z_tiles == 0 && a.sk_partials && a.sk_counters && a.schedule != 2 && a.schedule != 1) {
         // Split every tile of a small volume (fewer tiles than half a wave), or the tiles of a
         // partial last wave of a large one, over P CTAs of at least kBatch stages each, so that the
         // GPU stays full. Not HERCULES, whose small frames the batched kernel runs whole.
@@ -1287,7 +1288,7 @@ bool launch_das_k(const DasArgs& a, const void* iq, void* volume, cudaStream_t s
             return true;
         }
     }
-    if (!a.tiles && a.sk_partials && a.sk_counters) {
+    if (!a.tiles && a.z_tiles == 0 && a.sk_partials && a.sk_counters) {
         // More than one wave of tiles that is not a whole number of waves: the stream-K form
         // spreads the last, partly empty wave's work over every CTA.
         auto skern = das_stream_kernel<SEQ, CUBIC, CF, APO, IQ, SHORT, DB>;

@@ -352,6 +352,26 @@ CUTB_API bool cutb_plan_das_tile_shape(const cutb_plan* p, uint shape[3])
     return true;
 }
 
+CUTB_API bool cutb_das_zslab(cutb_plan* p, const void* d_iq, void* d_slab, uint z0, uint z1, void* stream)
+{
+    CUTB_REQUIRE(p, CUTB_ERR_INVALID_ARGUMENT, "Null plan.");
+    CUTB_REQUIRE(d_iq && d_slab, CUTB_ERR_INVALID_ARGUMENT, "Null device buffer.");
+    CUTB_REQUIRE(das_staged(p->das), CUTB_ERR_UNSUPPORTED,
+                 "Z-slabs need the staged delay-and-sum (not the one-thread-per-voxel kernel).");
+    int shape[3];
+    das_tile_shape(p->das, shape);
+    const uint Z = (uint)p->das.Z, tz = (uint)shape[2];
+    CUTB_REQUIRE(z0 < z1 && z1 <= Z && z0 % tz == 0 && (z1 % tz == 0 || z1 == Z), CUTB_ERR_INVALID_ARGUMENT,
+                 "Z-slab [%u, %u) must lie in [0, %u) with both ends on the tile depth %u (or the end at %u).", z0, z1,
+                 Z, tz, Z);
+    DasArgs a = p->das;
+    a.z_tile0 = (int)(z0 / tz);
+    a.z_tiles = (int)div_up(z1 - z0, tz);
+    a.z_out0 = (int)z0;
+    p->launches = 0;
+    return launch_das(a, d_iq, p->iq_bf16, d_slab, (cudaStream_t)stream, &p->launches);
+}
+
 CUTB_API bool cutb_das_tiles(cutb_plan* p, const void* d_iq, void* d_volume, const int* tiles, uint ntiles,
                              uint splits, void* stream)
 {

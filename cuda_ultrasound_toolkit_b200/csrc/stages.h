@@ -111,6 +111,8 @@ struct DasArgs {
     float4* sk_partials;       // stream-K scratch: 2 x kTileVoxels partial sums per pair of CTAs (null: off)
     int* sk_counters;          // stream-K: arrivals per pair of CTAs, zeroed before each launch
     int sk_capacity;           // pairs the scratch holds
+    int z_tile0, z_tiles;      // z-slab: tiles z_tile0 .. z_tile0 + z_tiles - 1 along z only (z_tiles 0: all)
+    int z_out0;                // voxel z of the output buffer's first plane (the slab's start)
     long long wait_limit;      // cycles a bounded wait spins before giving up (0: about 0.2 s)
     int debug_skip;            // test hook: stage debug_skip - 1 is never issued (0: off)
 };

@@ -112,6 +112,15 @@ CUTB_API bool cutb_beamform(cutb_plan* plan, const void* d_raw, size_t raw_bytes
  * with nx = ceil(X / shape[0]) etc. (1, 1, 1) for the one-thread-per-voxel kernel. */
 CUTB_API bool cutb_plan_das_tile_shape(const cutb_plan* plan, uint shape[3]);
 
+/* Delay-and-sum of the z-planes z0 .. z1 - 1 of the volume into d_slab [(z1 - z0)][Y][X] (complex64):
+ * the tiles of that depth range, unchanged, so slabs of one frame computed on several GPUs and put
+ * side by side equal cutb_das of the whole frame. z0 and z1 lie on the tile depth
+ * (cutb_plan_das_tile_shape; z1 may also be Z). It serves the sharding of one large frame over
+ * several GPUs: every GPU decodes and transforms the whole frame and beamforms its own slab
+ * (cuda_ultrasound_toolkit_b200/sharded.py). Staged engine only. No counterpart upstream, whose
+ * beamformer runs on one GPU (rf_processor.cpp:47). */
+CUTB_API bool cutb_das_zslab(cutb_plan* plan, const void* d_iq, void* d_slab, uint z0, uint z1, void* stream);
+
 /* Delay-and-sum of the listed tiles only (host array of tile ids), each tile's transmit x channel
  * stages split over `splits` CTAs whose partial sums are added atomically, so that a small set of
  * tiles still fills the GPU. d_volume [Z][Y][X] is cleared first; voxels outside the listed tiles
