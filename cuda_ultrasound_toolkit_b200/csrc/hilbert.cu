@@ -13,11 +13,15 @@
 // Z = DFT(x_a + i x_b):
 //   IDFT(Z Ge) = Re(iq_a) + i Re(iq_b),  IDFT(Z Go) = Im(iq_a) + i Im(iq_b),
 // because x_a, x_b are real (their spectra are Hermitian) and so are Ge, Go. That is 1.5
-// complex FFTs per row instead of 2, with no separation step. Ge, Go and the twiddles are
-// precomputed in FP64 on the host and stored as FP32 tables. A thread reads two twiddles per
-// radix-16 pass once, at the start (all three transforms share them), and forms the pass's
-// 15 twiddles as products of those: a per-butterfly table read per twiddle had kept the
-// load/store unit saturated (0.73 ms -> 0.31 ms on 16384 rows of 4096 samples).
+// complex FFTs per row instead of 2, with no separation step. The two inverse transforms run
+// together on paired FP32 lanes (lane 0: Z Ge, lane 1: Z Go; one instruction for both), so that
+// element n of the paired result is (Re iq_a, Im iq_a), (Re iq_b, Im iq_b): the output samples
+// themselves. Ge, Go and the twiddles are precomputed in FP64 on the host and stored as FP32
+// tables. A thread reads two twiddles per radix-16 pass once, at the start (all transforms share
+// them), and forms the pass's 15 twiddles as products of those: a per-butterfly table read per
+// twiddle had kept the load/store unit saturated (0.73 ms -> 0.31 ms on 16384 rows of 4096
+// samples); the paired inverse then took the kernel from 3 to 2 transforms' worth of
+// instructions per row pair.
 #include <atomic>
 #include <cmath>
 #include <complex>
@@ -53,6 +57,23 @@ __device__ __forceinline__ void run_fft(cplx (&x)[16], uint32_t tau, const cplx*
     }
 }
 
+// Two transforms at once on paired FP32 lanes (fft::fft_pass2), exchanging through float2 arrays.
+template <int LOGN, int SIGN, int P = 0>
+__device__ __forceinline__ void run_fft2(fft::cplx2 (&x)[16], uint32_t tau, const cplx* tw, float2* sre, float2* sim,
+                                         uint32_t skew, const fft::BaseTwiddles<LOGN>& wb)
+{
+    constexpr int NP = fft::pass_count(LOGN);
+    if constexpr (P < NP) {
+        fft::fft_pass2<LOGN, P, SIGN>(x, tau, tw, sre, sim, skew, wb);
+        if constexpr (P < NP - 1) {
+            __syncthreads();
+            fft::fft_gather2<LOGN>(x, tau, sre, sim, skew);
+            __syncthreads();
+        }
+        run_fft2<LOGN, SIGN, P + 1>(x, tau, tw, sre, sim, skew, wb);
+    }
+}
+
 // Writes output sample i (streaming: it is not read again by this kernel).
 __device__ __forceinline__ void store_iq(float2* out, uint64_t i, float re, float im)
 {
@@ -67,8 +88,8 @@ template <int LOGN>
 constexpr int hilbert_threads() { return hilbert_fft_per_block<LOGN>() * (1 << LOGN) / 16; }
 template <int LOGN>
 constexpr int hilbert_min_blocks() { return hilbert_threads<LOGN>() <= 256 ? 2 : 1; }
-// At 2^14 points the pair form needs 256 KiB of shared memory (exchange buffers + the held
-// product), above the 227 KiB a CTA may have; one row per CTA needs only the exchange buffers.
+// At 2^14 points the pair form needs 256 KiB of shared memory (the paired exchange buffers),
+// above the 227 KiB a CTA may have; one row per CTA needs half of that.
 template <int LOGN>
 constexpr bool hilbert_single_row() { return LOGN >= 14; }
 template <int LOGN>
@@ -76,7 +97,7 @@ constexpr size_t hilbert_smem_bytes()
 {
     constexpr size_t N = size_t(1) << LOGN;
     return hilbert_fft_per_block<LOGN>() *
-           (2 * fft::spad_size(N) * sizeof(float) + (hilbert_single_row<LOGN>() ? 0 : N * sizeof(float2)));
+           (hilbert_single_row<LOGN>() ? 2 * fft::spad_size(N) * sizeof(float) : 2 * N * sizeof(float2));
 }
 static_assert(hilbert_smem_bytes<14>() <= 227 * 1024 && hilbert_smem_bytes<13>() <= 227 * 1024, "shared memory");
 
@@ -99,7 +120,9 @@ hilbert_kernel(const float* __restrict__ in, OutT* __restrict__ out, HilbertArgs
     const uint64_t pair = (uint64_t)blockIdx.x * FPB + grp;
     const uint64_t ra = SINGLE ? (uint64_t)blockIdx.x : 2 * pair, rb = ra + 1;
     const bool has_a = ra < a.rows, has_b = !SINGLE && rb < a.rows;
-    float* sre = smem + grp * 2 * PN;
+    // Exchange arrays of the scalar transforms: the start of this row's region (the paired inverse
+    // reuses the whole region as two float2 arrays).
+    float* sre = smem + grp * (SINGLE ? 2 * PN : 4 * N);
     float* sim = sre + PN;
     const cplx* tw = reinterpret_cast<const cplx*>(a.twiddle);
 
@@ -115,19 +138,15 @@ hilbert_kernel(const float* __restrict__ in, OutT* __restrict__ out, HilbertArgs
     }
     run_fft<LOGN, -1>(z, tau, tw, sre, sim, wb);  // z[m] = Z[tau + m*TPF]
 
-    const float2* ge = reinterpret_cast<const float2*>(a.ge);
-    const float2* go = reinterpret_cast<const float2*>(a.go);
-    auto weight = [](const float2* t, uint32_t k) {
-        const float2 v = __ldg(t + k);
-        return cplx{v.x, v.y};
-    };
+    // Spectral weight per bin k: (Ge.re, Go.re, Ge.im, Go.im).
+    const float4* wt = reinterpret_cast<const float4*>(a.weight);
     if constexpr (SINGLE) {
         // One real row: iq = IDFT(X G) with G = Ge + i Go.
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             const uint32_t k = tau + m * TPF;
-            const cplx e = weight(ge, k), o = weight(go, k);
-            z[m] = fft::cmul(z[m], cplx{e.x - o.y, e.y + o.x});
+            const float4 w = __ldg(wt + k);
+            z[m] = fft::cmul(z[m], cplx{w.x - w.w, w.z + w.y});
         }
         run_fft<LOGN, +1>(z, tau, tw, sre, sim, wb);
 #pragma unroll
@@ -135,37 +154,30 @@ hilbert_kernel(const float* __restrict__ in, OutT* __restrict__ out, HilbertArgs
             const uint64_t n = tau + m * TPF;
             if (has_a && (!PAD || n < L)) store_iq(out, ra * L + n, z[m].x, z[m].y);
         }
-        return;
     } else {
-    // IDFT(Z Ge) = Re(iq_a) + i Re(iq_b) and IDFT(Z Go) = Im(iq_a) + i Im(iq_b). Z Go waits in this
-    // thread's own slots of `keep` while the first inverse transform runs, then the first result
-    // waits there during the second, and every output sample is written once, whole. Only one
-    // 16-element array is live at a time.
-    float2* keep = reinterpret_cast<float2*>(smem + FPB * 2 * PN) + grp * N;
+        // Lane 0: Z Ge, lane 1: Z Go, each cmul(z, weight) = {fma(z.x, w.x, -z.y w.y), fma(z.x, w.y, z.y w.x)};
+        // the paired inverse then leaves (Re iq_a, Im iq_a) in .re and (Re iq_b, Im iq_b) in .im.
+        fft::cplx2 y[16];
 #pragma unroll
-    for (int m = 0; m < 16; ++m) {
-        const uint32_t k = tau + m * TPF;
-        const cplx o = fft::cmul(z[m], weight(go, k));
-        keep[k] = make_float2(o.x, o.y);
-        z[m] = fft::cmul(z[m], weight(ge, k));
-    }
-    run_fft<LOGN, +1>(z, tau, tw, sre, sim, wb);
+        for (int m = 0; m < 16; ++m) {
+            const uint32_t k = tau + m * TPF;
+            const float4 w = __ldg(wt + k);
+            const float2 zx = make_float2(z[m].x, z[m].x), zy = make_float2(z[m].y, z[m].y);
+            y[m].re = fft::fma2(zx, make_float2(w.x, w.y), fft::mul2(zy, make_float2(-w.z, -w.w)));
+            y[m].im = fft::fma2(zx, make_float2(w.z, w.w), fft::mul2(zy, make_float2(w.x, w.y)));
+        }
+        // The forward transform's last shared-memory reads ended at a barrier, so the paired
+        // buffers (which overlay its arrays) are free.
+        float2* s2re = reinterpret_cast<float2*>(smem) + grp * 2 * N;
+        const uint32_t skew = (grp * TPF) & 15u;
+        run_fft2<LOGN, +1>(y, tau, tw, s2re, s2re + N, skew, wb);
 #pragma unroll
-    for (int m = 0; m < 16; ++m) {
-        const uint32_t k = tau + m * TPF;
-        const float2 o = keep[k];
-        keep[k] = make_float2(z[m].x, z[m].y);
-        z[m] = cplx{o.x, o.y};
-    }
-    run_fft<LOGN, +1>(z, tau, tw, sre, sim, wb);
-#pragma unroll
-    for (int m = 0; m < 16; ++m) {
-        const uint64_t n = tau + m * TPF;
-        if (PAD && n >= L) continue;
-        const float2 r = keep[n];
-        if (has_a) store_iq(out, ra * L + n, r.x, z[m].x);
-        if (has_b) store_iq(out, rb * L + n, r.y, z[m].y);
-    }
+        for (int m = 0; m < 16; ++m) {
+            const uint64_t n = tau + m * TPF;
+            if (PAD && n >= L) continue;
+            if (has_a) store_iq(out, ra * L + n, y[m].re.x, y[m].re.y);
+            if (has_b) store_iq(out, rb * L + n, y[m].im.x, y[m].im.y);
+        }
     }
 }
 
@@ -247,7 +259,8 @@ unsigned hilbert_fft_length(unsigned n)
 bool hilbert_supported_length(unsigned n) { return hilbert_fft_length(n) != 0; }
 
 // Host tables, all computed in double and rounded once to float: twiddles exp(-2*pi*i*m/M) of the
-// FFT length M = hilbert_fft_length(n) and the Hermitian parts of the spectral weight.
+// FFT length M = hilbert_fft_length(n) and the Hermitian parts of the spectral weight, interleaved
+// per bin as (Ge.re, Go.re, Ge.im, Go.im) so that one 16-byte load gives both paired lanes.
 //
 // Power-of-two rows (M = n): the weight is G = w * F itself.
 //
@@ -261,7 +274,7 @@ bool hilbert_supported_length(unsigned n) { return hilbert_fft_length(n) != 0; }
 // which do not overlap when M >= 2n - 1; its spectral weight is DFT_M(h) / M (the kernel's inverse
 // transform is unnormalised). Only outputs 0..n-1 are kept.
 bool build_hilbert_tables(unsigned n, const float* taps, unsigned ntaps, std::vector<float>& twiddle,
-                          std::vector<float>& ge, std::vector<float>& go)
+                          std::vector<float>& weight)
 {
     const unsigned M = hilbert_fft_length(n);
     CUTB_REQUIRE(M != 0, CUTB_ERR_UNSUPPORTED,
@@ -304,16 +317,15 @@ bool build_hilbert_tables(unsigned n, const float* taps, unsigned ntaps, std::ve
         fft_fp64(g, -1);
         for (auto& v : g) v /= (double)M;
     }
-    ge.resize(2 * (size_t)M);
-    go.resize(2 * (size_t)M);
+    weight.resize(4 * (size_t)M);
     for (unsigned k = 0; k < M; ++k) {
         const cd gm = std::conj(g[(M - k) % M]);
         const cd e = 0.5 * (g[k] + gm);
         const cd o = (g[k] - gm) / cd(0.0, 2.0);
-        ge[2 * k] = (float)e.real();
-        ge[2 * k + 1] = (float)e.imag();
-        go[2 * k] = (float)o.real();
-        go[2 * k + 1] = (float)o.imag();
+        weight[4 * (size_t)k] = (float)e.real();
+        weight[4 * (size_t)k + 1] = (float)o.real();
+        weight[4 * (size_t)k + 2] = (float)e.imag();
+        weight[4 * (size_t)k + 3] = (float)o.imag();
     }
     return true;
 }

@@ -30,7 +30,7 @@ constexpr unsigned kStaticMaxSamples = 16384;
 static_assert(kStaticMaxSamples >= kMaxHilbertLength, "the array must hold the longest transform's tables");
 constexpr int kMaxDevices = 64;
 
-// twiddle | Ge | Go, kStaticMaxSamples complex values each.
+// twiddle (kStaticMaxSamples complex values) | spectral weight (kStaticMaxSamples x 4 floats).
 static __device__ __align__(256) float g_hilbert_tables[3 * 2 * kStaticMaxSamples];
 
 std::mutex g_setup_mutex;
@@ -72,15 +72,14 @@ extern "C" CUTB_API bool cutb_hilbert_static(const float* d_in, uint in_stride, 
                  "Sample count %u not supported by the FFT (powers of two up to %u, other lengths up to %u).",
                  samples, kMaxHilbertLength, kMaxHilbertLength / 2);
     CUTB_REQUIRE(ntaps == 0 || taps, CUTB_ERR_INVALID_ARGUMENT, "Null match filter.");
-    std::vector<float> tw, ge, go;  // host memory only
-    if (!build_hilbert_tables(samples, taps, ntaps, tw, ge, go)) return false;
+    std::vector<float> tw, weight;  // host memory only
+    if (!build_hilbert_tables(samples, taps, ntaps, tw, weight)) return false;
     float* tables = nullptr;
     if (!table_address(&tables)) return false;
     cudaStream_t st = (cudaStream_t)stream;
     const size_t n = tw.size();  // 2 floats per point of the FFT length (<= kStaticMaxSamples)
     CUTB_CUDA_OK(cudaMemcpyAsync(tables, tw.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
-    CUTB_CUDA_OK(cudaMemcpyAsync(tables + n, ge.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
-    CUTB_CUDA_OK(cudaMemcpyAsync(tables + 2 * n, go.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
+    CUTB_CUDA_OK(cudaMemcpyAsync(tables + n, weight.data(), 2 * n * sizeof(float), cudaMemcpyHostToDevice, st));
     HilbertArgs a{};
     a.rows = rows;
     a.n = samples;
@@ -88,7 +87,6 @@ extern "C" CUTB_API bool cutb_hilbert_static(const float* d_in, uint in_stride, 
     while ((1u << a.log_n) < n / 2) ++a.log_n;
     a.in_stride = in_stride;
     a.twiddle = tables;
-    a.ge = tables + n;
-    a.go = tables + 2 * n;
+    a.weight = tables + n;
     return launch_hilbert(a, d_in, d_iq, false, st);
 }

@@ -167,20 +167,18 @@ bool FrontEnd::set_filter(const float* taps, uint32_t ntaps)
                  ntaps, S);
     fft_ok = hilbert_supported_length(S);
     if (!fft_ok) return true;  // decode still works; the Hilbert stage reports the length
-    std::vector<float> tw, ge, go;
-    if (!build_hilbert_tables(S, taps, ntaps, tw, ge, go)) return false;
+    std::vector<float> tw, weight;
+    if (!build_hilbert_tables(S, taps, ntaps, tw, weight)) return false;
     if (!d_tables && !alloc_bytes((void**)&d_tables, 3 * tw.size() * sizeof(float))) return false;
     CUTB_CUDA_OK(cudaMemcpy(d_tables, tw.data(), tw.size() * sizeof(float), cudaMemcpyHostToDevice));
-    CUTB_CUDA_OK(cudaMemcpy(d_tables + tw.size(), ge.data(), ge.size() * sizeof(float), cudaMemcpyHostToDevice));
     CUTB_CUDA_OK(
-        cudaMemcpy(d_tables + 2 * tw.size(), go.data(), go.size() * sizeof(float), cudaMemcpyHostToDevice));
+        cudaMemcpy(d_tables + tw.size(), weight.data(), weight.size() * sizeof(float), cudaMemcpyHostToDevice));
     hil.rows = (uint64_t)T * C;
     hil.n = S;
     hil.log_n = 0;
     while ((1u << hil.log_n) < tw.size() / 2) ++hil.log_n;
     hil.twiddle = d_tables;
-    hil.ge = d_tables + tw.size();
-    hil.go = d_tables + 2 * tw.size();
+    hil.weight = d_tables + tw.size();  // 16-byte aligned: tw.size() is a multiple of 32
     return true;
 }
 

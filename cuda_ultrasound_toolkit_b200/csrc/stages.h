@@ -62,8 +62,8 @@ struct HilbertArgs {
     uint32_t log_n;            // FFT length 2^log_n = hilbert_fft_length(n): n, or >= 2 n - 1 for other lengths
     uint32_t in_stride;        // 1: packed floats, 2: real part of complex input
     const float* twiddle;      // device: 2^log_n complex exp(-2 pi i m / 2^log_n)
-    const float* ge;           // device: 2^log_n complex, Hermitian-even part of the spectral weight
-    const float* go;           // device: 2^log_n complex, Hermitian-odd part (divided by i)
+    const float* weight;       // device: per bin k < 2^log_n, (Ge.re, Go.re, Ge.im, Go.im): the Hermitian-even
+                               // part of the spectral weight and the Hermitian-odd part divided by i
 };
 
 // FFT length for rows of n samples: n itself for powers of two from 16, else the power of two
@@ -71,7 +71,7 @@ struct HilbertArgs {
 unsigned hilbert_fft_length(unsigned n);
 bool hilbert_supported_length(unsigned n);
 bool build_hilbert_tables(unsigned n, const float* taps, unsigned ntaps, std::vector<float>& twiddle,
-                          std::vector<float>& ge, std::vector<float>& go);
+                          std::vector<float>& weight);
 bool launch_hilbert(const HilbertArgs& a, const float* in, void* out, bool bf16, cudaStream_t st);
 
 // ---- delay and sum (das.cu) ----------------------------------------------------------------
