@@ -28,6 +28,12 @@ is charged to the learned path.
 
   python -m cuda_ultrasound_toolkit_b200.sparse train --phantoms 2048 --epochs 4 --out weights.npz
   python -m cuda_ultrasound_toolkit_b200.sparse evaluate --weights weights.npz --phantoms 256
+  python -m cuda_ultrasound_toolkit_b200.sparse analyze --phantoms 16 --ab-phantoms 1024
+
+`analyze` measures where the restored volume's error comes from: the NRMSE on point-only and
+speckle-only phantoms, the best any linear per-depth filter along y (a global y-deconvolution) can
+do on held-out phantoms, and, with --ab-phantoms, the U-Net trained on the sparse volume against the
+same U-Net trained on that filter's output.
 """
 import argparse
 import json
@@ -107,7 +113,15 @@ def nrmse(est, ref):
     return float(torch.linalg.vector_norm(est - ref) / torch.linalg.vector_norm(ref))
 
 
-def make_pairs(n, seed0, log=print):
+def phantom_part(seed, part):
+    """phantom(seed) restricted to its point targets ("points"), its speckle ("speckle"), or whole."""
+    rng = np.random.default_rng(seed)
+    npts = int(rng.integers(50, 401))
+    scat = synth.phantom(rng, npts, N_SPECKLE, box_xy=BOX_XY, z_range=Z_RANGE)
+    return scat[:npts] if part == "points" else scat[npts:] if part == "speckle" else scat
+
+
+def make_pairs(n, seed0, log=print, part="mixed"):
     """(sparse volumes, full volumes) for phantoms seed0 .. seed0 + n - 1, complex64 on the GPU."""
     Z, Y, X = GRID
     xs = torch.empty((n, Z, Y, X), dtype=torch.complex64, device="cuda")
@@ -115,7 +129,7 @@ def make_pairs(n, seed0, log=print):
     full, sparse = full_acquisition(), sparse_acquisition()
     t0 = time.time()
     for k in range(n):
-        scat = torch.from_numpy(phantom(seed0 + k)).cuda()
+        scat = torch.from_numpy(phantom_part(seed0 + k, part)).cuda()
         full.acquire(scat, 2 * (seed0 + k))
         full.volume(out=ys[k])
         sparse.acquire(scat, 2 * (seed0 + k) + 1)
@@ -338,6 +352,114 @@ def evaluate(net, n, seed0=EVAL_SEED0, warmup=2, log=print):
     return summarize(rows), rows
 
 
+# ---- Where the error comes from -------------------------------------------------------------
+def y_filter_columns(v, k, half, depths):
+    """Regressors of output depth k: v[:, k + a, y + o, x] for a in depths, o = -half .. half (zero
+    outside the volume), one row per (volume, x, y)."""
+    Z, Y, X = GRID
+    cols = []
+    for a in depths:
+        if not 0 <= k + a < Z:
+            cols.append(torch.zeros((v.shape[0] * X * Y, 2 * half + 1), dtype=v.dtype, device=v.device))
+            continue
+        p = torch.nn.functional.pad(torch.view_as_real(v[:, k + a]).permute(0, 3, 2, 1), (half, half))
+        u = p.unfold(3, 2 * half + 1, 1)  # [n][2][X][Y][taps]
+        cols.append(torch.complex(u[:, 0], u[:, 1]).reshape(-1, 2 * half + 1))
+    return torch.cat(cols, 1)
+
+
+def fit_y_filter(xs, ys, half, depths, ridge=1e-3):
+    """Complex taps per output depth minimising sum |ys - filter(xs)|^2 (ridge relative to the
+    Gram matrix's mean diagonal): the best linear mixing along y (and nearby depths) there is."""
+    taps = []
+    for k in range(GRID[0]):
+        A = y_filter_columns(xs, k, half, depths)
+        t = ys[:, k].permute(0, 2, 1).reshape(-1)
+        G = A.conj().T @ A
+        G += ridge * torch.trace(G).real / G.shape[0] * torch.eye(G.shape[0], device=G.device)
+        taps.append(torch.linalg.solve(G, A.conj().T @ t))
+    return taps
+
+
+def apply_y_filter(v, taps, half, depths, chunk=32):
+    Z, Y, X = GRID
+    out = torch.empty_like(v)
+    for c in range(0, v.shape[0], chunk):
+        vc = v[c:c + chunk]
+        for k in range(Z):
+            out[c:c + chunk, k] = (y_filter_columns(vc, k, half, depths) @ taps[k]).reshape(-1, X, Y).permute(0, 2, 1)
+    return out
+
+
+def median_nrmse(xs, ys):
+    return float(np.median([nrmse(xs[k], ys[k]) for k in range(xs.shape[0])]))
+
+
+def train_on(xs, ys, hx, hy, epochs, batch=2, lr=1e-3, seed=1, log=print, tag=""):
+    """Trains a fresh U-Net on the pairs (xs, ys) with the schedule of `train`; returns the held-out
+    median NRMSE on (hx, hy) after each epoch."""
+    net = learn.UNet(GRID, max_batch=batch, seed=seed)
+    n = xs.shape[0]
+    steps, step, curve = epochs * (n // batch), 0, []
+    gen = torch.Generator(device="cpu").manual_seed(seed)
+    for ep in range(epochs):
+        perm = torch.randperm(n, generator=gen)
+        for b in range(n // batch):
+            idx = perm[b * batch:(b + 1) * batch].cuda()
+            net.train_step(xs.index_select(0, idx), ys.index_select(0, idx),
+                           lr * 0.5 * (1 + math.cos(math.pi * step / steps)))
+            step += 1
+        curve.append(held_out_nrmse(net, hx, hy)[0])
+        log(f"{tag}epoch {ep + 1}: held-out NRMSE median {curve[-1]:.4f}")
+    net.check()
+    net.close()
+    return curve
+
+
+def analyze(args, log=print):
+    """Prints (and returns) the measurements behind the learned path's error floor."""
+    res = {}
+    net = load(args.weights)
+    n = args.phantoms
+    parts = {}
+    for part in ("mixed", "points", "speckle"):
+        xs, ys = make_pairs(n, EVAL_SEED0, log=lambda *a: None, part=part)
+        out, vals = torch.empty_like(xs[:1]), []
+        for k in range(n):
+            net.forward(xs[k:k + 1], out=out)
+            vals.append(nrmse(out[0], ys[k]))
+        res[part] = dict(sparse=median_nrmse(xs, ys), unet=float(np.median(vals)))
+        log(f"{part:8s} phantoms: sparse volume NRMSE {res[part]['sparse']:.4f}, restored {res[part]['unet']:.4f}")
+        parts[part] = ys
+        del xs
+    share = [float(torch.linalg.vector_norm(parts["speckle"][k]) ** 2 /
+                   (torch.linalg.vector_norm(parts["points"][k]) ** 2 + torch.linalg.vector_norm(parts["speckle"][k]) ** 2))
+             for k in range(n)]
+    res["speckle_energy_share"] = float(np.median(share))
+    log(f"speckle share of the full volume's energy: median {res['speckle_energy_share']:.3f}")
+    del parts
+    fx, fy = make_pairs(n, EVAL_SEED0, log=lambda *a: None)
+    hx, hy = make_pairs(n, EVAL_SEED0 + 5000, log=lambda *a: None)
+    res["y_filter"] = []
+    for half, depths in ((0, (0,)), (16, (0,)), (48, (0,)), (96, (0,)), (48, (-1, 0, 1)), (48, (-3, -2, -1, 0, 1, 2, 3))):
+        taps = fit_y_filter(fx, fy, half, depths)
+        e = median_nrmse(apply_y_filter(hx, taps, half, depths), hy)
+        res["y_filter"].append(dict(half_width=half, depths=list(depths), held_out_nrmse=e))
+        log(f"linear filter along y, {2 * half + 1} taps x {len(depths)} depths: held-out NRMSE {e:.4f} "
+            f"(sparse volume {median_nrmse(hx, hy):.4f})")
+    del fx, fy, hx, hy
+    if args.ab_phantoms:
+        half, depths = 48, (-1, 0, 1)
+        xs, ys = make_pairs(args.ab_phantoms, TRAIN_SEED0, log)
+        hx, hy = make_pairs(64, EVAL_SEED0 + 500_000, log=lambda *a: None)
+        taps = fit_y_filter(xs[:64], ys[:64], half, depths)
+        res["ab_plain"] = train_on(xs, ys, hx, hy, args.ab_epochs, log=log, tag="U-Net on the sparse volume: ")
+        xs = apply_y_filter(xs, taps, half, depths)
+        res["ab_y_filtered"] = train_on(xs, ys, apply_y_filter(hx, taps, half, depths), hy, args.ab_epochs, log=log,
+                                        tag="U-Net on the y-filtered volume: ")
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -355,7 +477,19 @@ def main():
     e.add_argument("--weights", default=WEIGHTS)
     e.add_argument("--phantoms", type=int, default=256)
     e.add_argument("--json", default=None)
+    n = sub.add_parser("analyze")
+    n.add_argument("--weights", default=WEIGHTS)
+    n.add_argument("--phantoms", type=int, default=16)
+    n.add_argument("--ab-phantoms", type=int, default=0, help="also train the A/B pair on this many phantoms")
+    n.add_argument("--ab-epochs", type=int, default=4)
+    n.add_argument("--json", default=None)
     a = ap.parse_args()
+    if a.cmd == "analyze":
+        res = analyze(a)
+        if a.json:
+            with open(a.json, "w") as f:
+                json.dump(res, f)
+        return
     if a.cmd == "train":
         net = train(a)
         if a.eval:
