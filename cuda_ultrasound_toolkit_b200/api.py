@@ -275,7 +275,7 @@ def corr_images_device(template, source, out=None, stream=None):
 # ---- device-resident stages ----------------------------------------------------------------------
 class _Options(ctypes.Structure):
     _fields_ = [("iq_bf16", ctypes.c_int), ("das_tile", ctypes.c_int), ("decode_tc", ctypes.c_int),
-                ("das_schedule", ctypes.c_int), ("reserved", ctypes.c_int * 12)]
+                ("das_schedule", ctypes.c_int), ("das_rows_per_stage", ctypes.c_int), ("reserved", ctypes.c_int * 11)]
 
 
 def _stream_handle(stream):
@@ -289,10 +289,11 @@ class Plan:
     """cutb_plan over torch CUDA tensors. Stage calls are asynchronous on `stream`
     (default: the current torch stream)."""
 
-    def __init__(self, bp: CudaBeamformerParameters, iq_bf16=False, das_tile=0, decode_tc=False, das_schedule=0):
+    def __init__(self, bp: CudaBeamformerParameters, iq_bf16=False, das_tile=0, decode_tc=False, das_schedule=0,
+                 das_rows_per_stage=0):
         import torch  # noqa: F401  (device memory comes from torch)
         self.bp = bp.copy()
-        opts = _Options(int(iq_bf16), int(das_tile), int(decode_tc), int(das_schedule))
+        opts = _Options(int(iq_bf16), int(das_tile), int(decode_tc), int(das_schedule), int(das_rows_per_stage))
         self._L = lib()
         self._h = self._L.cutb_plan_create(ctypes.byref(self.bp), ctypes.byref(opts))
         _check(self._h, "cutb_plan_create")

@@ -239,14 +239,22 @@ struct Tile {
 struct StageId {
     int t, g, c0, nq;
 };
+// Receive channels per stage (cutb_options.das_rows_per_stage): at most kRows, the rows the
+// stage buffers hold; a stage of fewer rows leaves the rest of its buffer unused.
+__host__ __device__ __forceinline__ int stage_rows(const DasArgs& a)
+{
+    return a.rows_per_stage > 0 && a.rows_per_stage < kRows ? a.rows_per_stage : kRows;
+}
+
 __device__ __forceinline__ StageId stage_id(const DasArgs& a, int k, int nchunks)
 {
     StageId s;
     s.g = k % a.G;
     const int chunk = (k / a.G) % nchunks;
     s.t = k / (a.G * nchunks);
-    s.c0 = chunk * kRows;
-    s.nq = min(kRows, a.C - s.c0);
+    const int rows = stage_rows(a);
+    s.c0 = chunk * rows;
+    s.nq = min(rows, a.C - s.c0);
     return s;
 }
 
@@ -756,7 +764,7 @@ static_assert(kTileVoxels == (int)kStreamTileVoxels, "stream-K scratch holds one
 // (row 0 is the flash; used transmit t reads row t + 1).
 __host__ __device__ __forceinline__ int tile_stages(const DasArgs& a)
 {
-    return (a.seq == UFORCES ? a.T - 1 : a.T) * div_up(a.C, kRows) * a.G;
+    return (a.seq == UFORCES ? a.T - 1 : a.T) * div_up(a.C, stage_rows(a)) * a.G;
 }
 
 // One tile (bx, by, bz) of the volume, stages k_lo .. k_hi - 1. Called by the grid
@@ -880,7 +888,7 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
         }
     }
 
-    const int nchunks = div_up(a.C, kRows);
+    const int nchunks = div_up(a.C, stage_rows(a));
     const int k_begin = k_lo, nstages = k_hi;
     // Window metadata (FP64) is computed for kBatch stages at a time by all threads; a stage's
     // bulk copies are then issued by lanes 0..kRows-1 of warp 0, one row per lane.

@@ -487,6 +487,9 @@ bool cutb_plan::build(const CudaBeamformerParameters& params, const cutb_options
     CUTB_REQUIRE(opt.das_schedule >= 0 && opt.das_schedule <= 2, CUTB_ERR_INVALID_ARGUMENT,
                  "Unknown delay-and-sum schedule %d.", opt.das_schedule);
     das.schedule = opt.das_schedule;
+    CUTB_REQUIRE(opt.das_rows_per_stage >= 0 && opt.das_rows_per_stage <= 8, CUTB_ERR_INVALID_ARGUMENT,
+                 "Rows per delay-and-sum stage must be 1..8 (0: 8), not %d.", opt.das_rows_per_stage);
+    das.rows_per_stage = opt.das_rows_per_stage;
     if (das.seq == RCA_TPW) {  // beamformer.cu:439-443: angle of transmit t in foci[t][2], radians
         std::vector<float> angles(das.T);
         for (int t = 0; t < das.T; ++t) angles[t] = bp.foci[3 * t + 2];

@@ -104,6 +104,7 @@ struct DasArgs {
     int tile;                  // 0 chosen from the grid, 1 = 4 x 8 x 32, 2 = 8 x 8 x 16 (HERCULES, TPW in a
                                // y-z plane), 3 = one thread per voxel (TPW, UFORCES)
     int schedule;              // 0: split partial last wave / small 2-D volumes, 1: one CTA per tile, 2: stream-K
+    int rows_per_stage;        // staged engine: receive channels per stage, 1 .. 8 (0: 8)
     const int* tiles;          // optional device list of tile ids (z-major); null = every tile
     int ntiles;
     int splits;                // > 1: stages split across CTAs, partial sums added atomically

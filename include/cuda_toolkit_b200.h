@@ -72,7 +72,9 @@ typedef struct cutb_options {
                          wave) over several CTAs whose partial sums meet in plan-owned scratch
                          memory; 1 = one CTA per tile; 2 = stream-K when the tiles exceed one wave
                          (the last waves' tiles x stages split evenly over the resident CTAs) */
-    int reserved[12];
+    int das_rows_per_stage; /* staged delay-and-sum: receive channels per TMA stage, 1..8 (0 = 8);
+                               fewer rows mean more stages and block barriers per channel */
+    int reserved[11];
 } cutb_options;
 
 typedef struct cutb_plan cutb_plan;

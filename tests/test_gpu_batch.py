@@ -9,7 +9,7 @@ import pytest
 import torch
 
 from cuda_ultrasound_toolkit_b200 import Batch, Plan, batched
-from cuda_ultrasound_toolkit_b200.tune import DasTuner, CANDIDATES, candidates
+from cuda_ultrasound_toolkit_b200.tune import DasTuner, candidates, schedules
 
 pytestmark = pytest.mark.gpu
 
@@ -98,12 +98,23 @@ def test_tuner_choice_is_fastest_on_remeasure(tmp_path):
     spec = dict(T=32, C=64, S=2048, X=64, Y=64, Z=64, scatterers=50, seed=9)
     bp = batched.make_frames([spec])[0][1]
     tuner = DasTuner(str(tmp_path / "tiles.json"), reps=3)
-    best = tuner.choose(bp)
-    times = {t: tuner.measure(bp, t, reps=5) for t in CANDIDATES}
-    assert times[best] <= 1.1 * min(times.values()), times
+    cfg = tuner.choose_config(bp)
+    entry = tuner.entry(bp)
+    # every tile x schedule was timed, and rows per stage at the best of them
+    assert {f"tile{t}/schedule{s}/rows0" for t in candidates(bp) for s in schedules(bp, t)} <= set(entry["ms"])
+    assert any(k.endswith("rows4") for k in entry["ms"])
+    times = {(t, s): tuner.measure(bp, t, schedule=s, reps=5) for t in candidates(bp) for s in schedules(bp, t)}
+    chosen = tuner.measure(bp, cfg["das_tile"], schedule=cfg["das_schedule"], rows=cfg["das_rows_per_stage"], reps=5)
+    assert chosen <= 1.1 * min(times.values()), (cfg, chosen, times)
+    # 32 transmits and 2048 samples: both decode engines run; the faster one is kept
+    assert set(entry["decode_ms"]) == {"False", "True"}
+    dec = {tc: tuner.measure_decode(bp, tc, reps=5) for tc in (False, True)}
+    assert dec[cfg["decode_tc"]] <= 1.15 * min(dec.values()), (cfg, dec)
+    assert tuner.choose(bp) == cfg["das_tile"]
     # persisted and reloaded without measuring again
     again = DasTuner(str(tmp_path / "tiles.json"))
-    assert again.choose(bp) == best
+    assert again.choose_config(bp) == cfg
+    Plan(bp, **cfg).close()
 
 
 @pytest.mark.parametrize("half", [19.2e-3, 2.4e-3])  # a coarse grid over the aperture, a fine one
@@ -120,7 +131,8 @@ def test_tuner_picks_the_engine_for_tpw(tmp_path, half):
     for t, a in enumerate(np.linspace(-0.2, 0.2, 32)):
         bp.foci[3 * t + 2] = float(a)
     tuner = DasTuner(str(tmp_path / "tiles.json"), reps=3)
-    best = tuner.choose(bp)
-    assert best in candidates(bp) == (2, 3)
-    times = {t: tuner.measure(bp, t, reps=5) for t in candidates(bp)}
-    assert times[best] <= 1.15 * min(times.values()), times
+    cfg = tuner.choose_config(bp)
+    assert cfg["das_tile"] in candidates(bp) == (2, 3)
+    times = {(t, s): tuner.measure(bp, t, schedule=s, reps=5) for t in candidates(bp) for s in schedules(bp, t)}
+    chosen = tuner.measure(bp, cfg["das_tile"], schedule=cfg["das_schedule"], rows=cfg["das_rows_per_stage"], reps=5)
+    assert chosen <= 1.15 * min(times.values()), (cfg, chosen, times)
