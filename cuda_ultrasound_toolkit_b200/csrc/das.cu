@@ -210,6 +210,10 @@ struct alignas(128) Smem {
     float4 coefA[NC >= 1 ? kCB : 1][NC >= 1 ? kRows : 1][NC >= 1 ? kWin : 1];
     float4 coefB[NC == 2 ? kCB : 1][NC == 2 ? kRows : 1][NC == 2 ? kWin : 1];
     RowMeta rowc[NC >= 1 ? kCB : 1][NC >= 1 ? kRows : 1];  // metadata of the rows whose coefficients are built
+    // The fields of rowc that the packed row pass reads for every row, (ex2, d0sq, d0, base): one
+    // 16-byte warp-uniform load (2 shared-memory wavefronts) instead of five 4-byte loads of the
+    // 56-byte RowMeta (5 wavefronts), about 5 % of the kernel's wavefronts on the benchmark frame.
+    float4 rowk[NC >= 1 ? kCB : 1][NC >= 1 ? kRows : 1];
     RowMeta row[kStages][kRows];
     StageMeta stage[kStages];
     RowMeta next_row[kSlots][kRows];    // precomputed metadata of upcoming stages (ring)
@@ -223,6 +227,10 @@ struct alignas(128) Smem {
     int tx_reach_bits;
     int part_last;  // stream-K: the pair counter's value before this part's arrival
 };
+
+// The double-buffered form runs three CTAs per SM: 228 KiB of shared memory per SM, 1 KiB of it
+// reserved per CTA.
+static_assert(3 * (sizeof(Smem<float2, 2, true>) + 1024) <= 228 * 1024, "three double-buffered CTAs per SM");
 
 // Coefficient arrays staged per row: cubic always 2; linear 1 where the packed row pass runs
 // (HERCULES without apodization), else 0 (the taps are read from the raw windows).
@@ -493,7 +501,11 @@ template <class IQ, int NC, bool DB>
 __device__ __forceinline__ void build_coefficients(Smem<IQ, NC, DB>& sm, int b, int nq, int cb, int wint,
                                                    float rwint, int first, int count, const float2* rot_tab = nullptr)
 {
-    if (threadIdx.x < nq) sm.rowc[cb][threadIdx.x] = sm.row[b][threadIdx.x];
+    if (threadIdx.x < nq) {
+        const RowMeta m = sm.row[b][threadIdx.x];
+        sm.rowc[cb][threadIdx.x] = m;
+        sm.rowk[cb][threadIdx.x] = make_float4(m.ex2, m.d0sq, m.d0, m.base);
+    }
     const int n = nq * wint;
     if ((int)threadIdx.x < first) return;
 #pragma unroll 1
@@ -686,13 +698,15 @@ __device__ __forceinline__ void row_pass_packed(const Smem<IQ, NC, DB>& sm, int 
                                                 const f2x (&txs2)[kVpt / 2], f2x (&tot2)[kVpt], f2x (&inc2)[kVpt])
 {
     constexpr float kMagic = 8388608.f;
-    const RowMeta& m = rows[qi];
-    const float exdx = m.ex2 * dxe;
+    const float4 k = sm.rowk[cb][qi];  // (ex2, d0sq, d0, base) of rows[qi]
+    const float exdx = k.x * dxe;
     const f2x nexdx2 = pk(-exdx, -exdx);
-    const f2x d0sq2 = pk(m.d0sq, m.d0sq), nd02 = pk(-m.d0, -m.d0), td02 = pk(m.two_d0, m.two_d0);
-    const f2x base2 = pk(m.base, m.base), spm2 = pk(spm, spm), mhalf2 = pk(-0.5f, -0.5f);
+    // 2 d0 in FP32 equals the row's two_d0 (FP64 2 d0 rounded): doubling is exact
+    const f2x d0sq2 = pk(k.y, k.y), nd02 = pk(-k.z, -k.z), td02 = pk(2.f * k.z, 2.f * k.z);
+    const f2x base2 = pk(k.w, k.w), spm2 = pk(spm, spm), mhalf2 = pk(-0.5f, -0.5f);
     const f2x magic2 = pk(kMagic, kMagic);
-    const float loc = m.loclamp, hic = m.hiclamp;
+    float loc = 0.f, hic = 0.f;
+    if constexpr (CLAMP) loc = rows[qi].loclamp, hic = rows[qi].hiclamp;
     const float4* cA = sm.coefA[cb][qi];
     const float4* cB = sm.coefB[NC == 2 ? cb : 0][NC == 2 ? qi : 0];
 #pragma unroll
@@ -964,8 +978,10 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
             // taken per stage, not per row, so the unrolled row loop stays one straight-line block
             // in which the rows' independent delay chains interleave (a per-row branch measured 9%
             // slower; the full unroll of an 8-row stage 3% faster than unrolling by 2).
-            bool unclamped = all_staged;
-            for (int q = 0; q < st.nq; ++q) unclamped &= rows[q].unclamped != 0;
+            // every row of the stage unclamped: lane q reads row q's flag, one load per warp
+            const unsigned need = (1u << st.nq) - 1u;
+            const bool row_unclamped = lane < st.nq && rows[lane].unclamped != 0;
+            const bool unclamped = all_staged && (__ballot_sync(0xffffffffu, row_unclamped) & need) == need;
             if (unclamped && st.nq == kRows) {
 #pragma unroll
                 for (int qi = 0; qi < kRows; ++qi)
