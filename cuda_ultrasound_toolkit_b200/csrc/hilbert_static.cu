@@ -72,6 +72,13 @@ extern "C" CUTB_API bool cutb_hilbert_static(const float* d_in, uint in_stride, 
                  "Sample count %u not supported by the FFT (powers of two up to %u, other lengths up to %u).",
                  samples, kMaxHilbertLength, kMaxHilbertLength / 2);
     CUTB_REQUIRE(ntaps == 0 || taps, CUTB_ERR_INVALID_ARGUMENT, "Null match filter.");
+    // The table upload copies from host vectors that are freed when the call returns, so a graph
+    // captured from it would replay reads of freed memory: capture is refused.
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    CUTB_CUDA_OK(cudaStreamIsCapturing((cudaStream_t)stream, &capturing));
+    CUTB_REQUIRE(capturing == cudaStreamCaptureStatusNone, CUTB_ERR_UNSUPPORTED,
+                 "cutb_hilbert_static cannot be captured in a CUDA graph (its tables are uploaded from host "
+                 "memory that the call frees).");
     std::vector<float> tw, weight;  // host memory only
     if (!build_hilbert_tables(samples, taps, ntaps, tw, weight)) return false;
     float* tables = nullptr;

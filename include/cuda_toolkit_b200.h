@@ -181,9 +181,10 @@ CUTB_API int cutb_plan_last_launch_count(const cutb_plan* plan);
  * array sized for transforms of up to 16384 points (384 KiB, held by every GPU that loads the
  * library until the process exits): rows of up to 16384 samples when the count is a power of two,
  * up to 8192 otherwise. Rows longer than 16384 are rejected with CUTB_ERR_INVALID_ARGUMENT, other
- * unsupported counts with CUTB_ERR_UNSUPPORTED. The first call on a
- * device looks up that array's address, so make it before any stream capture. Every call rewrites
- * the array on `stream`; calls that overlap on the GPU race on it and must be serialised. */
+ * unsupported counts with CUTB_ERR_UNSUPPORTED. A call on a stream that is being captured into a
+ * CUDA graph is rejected with CUTB_ERR_UNSUPPORTED: the tables are uploaded from host memory that
+ * the call frees before a graph could replay the copy. Every call rewrites the array on `stream`;
+ * calls that overlap on the GPU race on it and must be serialised. */
 CUTB_API bool cutb_hilbert_static(const float* d_in, uint in_stride, void* d_iq, uint samples, size_t rows,
                                   const float* taps, uint ntaps, void* stream);
 

@@ -84,3 +84,21 @@ def test_static_hilbert_rejects_rows_beyond_capacity():
     buf = torch.zeros(16, dtype=torch.float32, device="cuda")
     assert not fn(buf.data_ptr(), 1, buf.data_ptr(), 32768, 1, None, 0, None)
     assert lib().cutb_last_error() == 1
+
+
+def test_static_hilbert_refuses_stream_capture():
+    """Its tables are uploaded from host memory that the call frees, so a captured call is refused."""
+    import torch
+    fn = _static_entry()
+    src = torch.zeros(4 * 256, dtype=torch.float32, device="cuda")
+    dst = torch.zeros(4 * 256, dtype=torch.complex64, device="cuda")
+    graph = torch.cuda.CUDAGraph()
+    stream = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    with torch.cuda.graph(graph, stream=stream):
+        ok = fn(src.data_ptr(), 1, dst.data_ptr(), 256, 4, None, 0, ctypes.c_void_p(stream.cuda_stream))
+        code = lib().cutb_last_error()
+    assert not ok and code == 2  # CUTB_ERR_UNSUPPORTED
+    # outside a capture the same call runs
+    assert fn(src.data_ptr(), 1, dst.data_ptr(), 256, 4, None, 0, None)
+    torch.cuda.synchronize()
