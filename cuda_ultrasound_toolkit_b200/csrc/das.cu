@@ -752,6 +752,83 @@ __device__ __forceinline__ void row_pass_packed(const Smem<IQ, NC, DB>& sm, int 
     }
 }
 
+// row_pass for TPW and UFORCES, cubic, staged rows, on packed FP32x2 instructions: the delay chain
+// of voxel pairs as in row_pass_packed (the receive path of the scalar pass, element by element),
+// the Horner evaluation and the accumulation in (re, im) pairs. The receive Hann window and the
+// rotation exp(i 2 pi fc/fs t) stay scalar (special-function unit). A window below 0.1 (TPW)
+// gives the voxel weight 0 instead of skipping it, which adds +-0 to its sums.
+template <int SEQ, bool CF, bool CLAMP, class IQ, int NC, bool DB>
+__device__ __forceinline__ void row_pass_packed_tu(const Smem<IQ, NC, DB>& sm, int cb, const RowMeta* rows, int qi,
+                                                   float dxe, float spm, float vx, float phi, float sign,
+                                                   float uni_apo, const f2x (&sq2)[kVpt / 2],
+                                                   const f2x (&tsh2)[kVpt / 2], const float (&vzv)[kVpt],
+                                                   f2x (&tot2)[kVpt], f2x (&inc2)[kVpt])
+{
+    static_assert(NC == 2, "cubic coefficients");
+    constexpr float kMagic = 8388608.f;
+    const float4 k = sm.rowk[cb][qi];  // (ex2, d0sq, d0, base) of rows[qi]
+    const float exdx = k.x * dxe;
+    const f2x nexdx2 = pk(-exdx, -exdx);
+    const f2x d0sq2 = pk(k.y, k.y), nd02 = pk(-k.z, -k.z), td02 = pk(2.f * k.z, 2.f * k.z);
+    const f2x base2 = pk(k.w, k.w), spm2 = pk(spm, spm), mhalf2 = pk(-0.5f, -0.5f);
+    const f2x magic2 = pk(kMagic, kMagic);
+    float loc = 0.f, hic = 0.f;
+    if constexpr (CLAMP) loc = rows[qi].loclamp, hic = rows[qi].hiclamp;
+    const float rxa = fabsf(rows[qi].xc - vx);
+    const float4* cA = sm.coefA[cb][qi];
+    const float4* cB = sm.coefB[cb][qi];
+#pragma unroll
+    for (int p = 0; p < kVpt / 2; ++p) {
+        const f2x nd = sub2(nexdx2, sq2[p]);  // -delta
+        const f2x D = sub2(d0sq2, nd);        // d0^2 + delta
+        float D0, D1;
+        upk(D, D0, D1);
+        const f2x r = pk(rsqrt_approx(D0), rsqrt_approx(D1));
+        const f2x e0 = fma2(D, r, nd02);
+        const f2x res = fma2(e0, add2(e0, td02), nd);
+        const f2x corr = fma2(mul2(mhalf2, r), res, e0);
+        f2x ic = fma2(corr, spm2, add2(base2, tsh2[p]));
+        if constexpr (CLAMP) {
+            float x0, x1;
+            upk(ic, x0, x1);
+            x0 = fminf(fmaxf(x0, loc), hic);
+            x1 = fminf(fmaxf(x1, loc), hic);
+            ic = pk(x0, x1);
+        }
+        const f2x f = add2_rm(ic, magic2);
+        float f0, f1;
+        upk(f, f0, f1);
+        const int i0 = __float_as_int(f0) - __float_as_int(kMagic);
+        const int i1 = __float_as_int(f1) - __float_as_int(kMagic);
+        float t0, t1;
+        upk(sub2(ic, sub2(f, magic2)), t0, t1);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int v = 2 * p + h;
+            const int i = h ? i1 : i0;
+            const float t = h ? t1 : t0;
+            // receive Hann window (vzv = fn_rx / (2 depth)), as the scalar pass
+            const float c = __cosf(kPi * fminf(rxa * vzv[v], 0.5f));
+            float apo = c * c;
+            if (Seq<SEQ>::kTpw && apo < 0.1f) apo = 0.f;
+            const float w = sign * (apo * uni_apo);
+            const float4 A = cA[i], B = cB[i];
+            const f2x tt = pk(t, t);
+            f2x val = fma2(fma2(fma2(pk(B.z, B.w), tt, pk(B.x, B.y)), tt, pk(A.z, A.w)), tt, pk(A.x, A.y));
+            if constexpr (Seq<SEQ>::kTpw) {  // the rest of the rotation, exp(i 2 pi fc/fs t), t in [0, 1)
+                float sn, cs, vr, vi;
+                __sincosf(phi * t, &sn, &cs);
+                upk(val, vr, vi);
+                const float2 rot = cmulf(make_float2(vr, vi), make_float2(cs, sn));
+                val = pk(rot.x, rot.y);
+            }
+            const f2x vw = mul2(val, pk(w, w));
+            tot2[v] = add2(tot2[v], vw);
+            if (CF) inc2[v] = fma2(vw, vw, inc2[v]);
+        }
+    }
+}
+
 // Thread layout. HERCULES: lanes are 4 (x) x 8 (y) neighbours, whose delays differ by less
 // than a sample or two, so their shared-memory reads fall in distinct banks or broadcast;
 // warps and the kVpt registers of a thread run along z. FORCES (no y): lanes along x.
@@ -888,16 +965,22 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
     // linear coefficients.
     constexpr bool PACKED = HERC && !APO;
     static_assert(!PACKED || NC > 0, "the packed pass reads coefficients");
+    // TPW and UFORCES with cubic interpolation accumulate staged rows on packed FP32x2 as well
+    // (row_pass_packed_tu); rows read from global memory take the scalar pass.
+    constexpr bool PACKED_TU = (Q::kTpw || Q::kUf) && CUBIC && !DB;
+    constexpr bool ANY_PACKED = PACKED || PACKED_TU;
     float2 total[kVpt];
     float inc[kVpt];
-    f2x tot2[PACKED ? kVpt : 1], inc2[PACKED ? kVpt : 1], txs2[PACKED ? kVpt / 2 : 1];
+    f2x tot2[ANY_PACKED ? kVpt : 1], inc2[ANY_PACKED ? kVpt : 1], txs2[PACKED ? kVpt / 2 : 1];
 #pragma unroll
     for (int v = 0; v < kVpt; ++v) {
         total[v] = make_float2(0.f, 0.f);
         inc[v] = 0.f;
-        if constexpr (PACKED) {
+        if constexpr (ANY_PACKED) {
             tot2[v] = 0ull;
             inc2[v] = 0ull;
+        }
+        if constexpr (PACKED) {
             if (v % 2 == 0) txs2[v / 2] = pk(txs[v], txs[v + 1]);
         }
     }
@@ -1003,6 +1086,37 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
                                                              tsh, vzv, vx, a2, total, inc);
                 }
             }
+        } else if constexpr (PACKED_TU) {
+            f2x sq2[kVpt / 2], tsh2[kVpt / 2];
+#pragma unroll
+            for (int p = 0; p < kVpt / 2; ++p) {
+                sq2[p] = pk(sq[2 * p], sq[2 * p + 1]);
+                tsh2[p] = pk(tsh[2 * p], tsh[2 * p + 1]);
+            }
+            const float phi = Q::kTpw ? (float)(6.283185307179586 * a.fc_fs) : 0.f;  // 2 pi fc/fs
+            const unsigned need = (1u << st.nq) - 1u;
+            const bool row_unclamped = lane < st.nq && rows[lane].unclamped != 0;
+            const bool unclamped = all_staged && (__ballot_sync(0xffffffffu, row_unclamped) & need) == need;
+            if (unclamped) {
+#pragma unroll 2
+                for (int qi = 0; qi < st.nq; ++qi)
+                    row_pass_packed_tu<SEQ, CF, false>(sm, cb, rows, qi, dxe, a.spm, vx, phi, st.sign, st.uni_apo, sq2,
+                                                       tsh2, vzv, tot2, inc2);
+            } else if (all_staged) {
+#pragma unroll 2
+                for (int qi = 0; qi < st.nq; ++qi)
+                    row_pass_packed_tu<SEQ, CF, true>(sm, cb, rows, qi, dxe, a.spm, vx, phi, st.sign, st.uni_apo, sq2,
+                                                      tsh2, vzv, tot2, inc2);
+            } else {
+                for (int qi = 0; qi < st.nq; ++qi) {
+                    if (rows[qi].len > 0)
+                        row_pass_packed_tu<SEQ, CF, true>(sm, cb, rows, qi, dxe, a.spm, vx, phi, st.sign, st.uni_apo,
+                                                          sq2, tsh2, vzv, tot2, inc2);
+                    else
+                        row_pass<SEQ, CUBIC, CF, APO, false>(a, sm, rows, b, qi, grow0 + (size_t)qi * a.S, st, dxe, sq,
+                                                             tsh, vzv, vx, a2, total, inc, rot_tab);
+                }
+            }
         } else if (all_staged) {
 #pragma unroll 2
             for (int qi = 0; qi < st.nq; ++qi)
@@ -1036,7 +1150,7 @@ __device__ __forceinline__ void das_tile(const IQ* __restrict__ iq, float2* __re
         return;
     }
 
-    if constexpr (PACKED) {
+    if constexpr (ANY_PACKED) {
 #pragma unroll
         for (int v = 0; v < kVpt; ++v) {
             float tx, ty, ix, iy;
