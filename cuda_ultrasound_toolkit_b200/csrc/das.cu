@@ -701,8 +701,7 @@ __device__ __forceinline__ void row_pass_packed(const Smem<IQ, NC, DB>& sm, int 
     const float4 k = sm.rowk[cb][qi];  // (ex2, d0sq, d0, base) of rows[qi]
     const float exdx = k.x * dxe;
     const f2x nexdx2 = pk(-exdx, -exdx);
-    // 2 d0 in FP32 equals the row's two_d0 (FP64 2 d0 rounded): doubling is exact
-    const f2x d0sq2 = pk(k.y, k.y), nd02 = pk(-k.z, -k.z), td02 = pk(2.f * k.z, 2.f * k.z);
+    const f2x d0sq2 = pk(k.y, k.y), nd02 = pk(-k.z, -k.z), mtwo2 = pk(-2.f, -2.f);
     const f2x base2 = pk(k.w, k.w), spm2 = pk(spm, spm), mhalf2 = pk(-0.5f, -0.5f);
     const f2x magic2 = pk(kMagic, kMagic);
     float loc = 0.f, hic = 0.f;
@@ -717,7 +716,8 @@ __device__ __forceinline__ void row_pass_packed(const Smem<IQ, NC, DB>& sm, int 
         upk(D, D0, D1);
         const f2x r = pk(rsqrt_approx(D0), rsqrt_approx(D1));
         const f2x e0 = fma2(D, r, nd02);
-        const f2x res = fma2(e0, add2(e0, td02), nd);
+        // e0 + 2 d0 as fma(-2, -d0, e0): the product is exact, so this is the sum with the row's two_d0
+        const f2x res = fma2(e0, fma2(mtwo2, nd02, e0), nd);
         const f2x corr = fma2(mul2(mhalf2, r), res, e0);
         f2x ic = fma2(corr, spm2, add2(base2, txs2[p]));
         if constexpr (CLAMP) {
