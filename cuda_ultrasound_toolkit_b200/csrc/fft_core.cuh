@@ -166,9 +166,23 @@ __host__ __device__ __forceinline__ void load_base_twiddles(BaseTwiddles<LOGN>& 
     }
 }
 
-template <int LOGN, int P, int SIGN>
-__host__ __device__ __forceinline__ void fft_pass(cplx (&x)[16], uint32_t tau, const cplx* __restrict__ tw,
-                                                  float* sre, float* sim, const BaseTwiddles<LOGN>& wb)
+// The exchange arrays of one transform: element `pos` (already swizzled) stored and loaded as
+// (re, im). ShmemPair: two float arrays in this CTA's shared memory; a cluster form spreads them
+// over the shared memory of several CTAs (hilbert.cu).
+struct ShmemPair {
+    float* re;
+    float* im;
+    __host__ __device__ __forceinline__ void store(uint32_t pos, cplx v) const
+    {
+        re[pos] = v.x;
+        im[pos] = v.y;
+    }
+    __host__ __device__ __forceinline__ cplx load(uint32_t pos) const { return {re[pos], im[pos]}; }
+};
+
+template <int LOGN, int P, int SIGN, class EX>
+__host__ __device__ __forceinline__ void fft_pass_ex(cplx (&x)[16], uint32_t tau, const cplx* __restrict__ tw,
+                                                     const EX& ex, const BaseTwiddles<LOGN>& wb)
 {
     constexpr int N = 1 << LOGN;
     constexpr int TPF = N / 16;
@@ -217,25 +231,31 @@ __host__ __device__ __forceinline__ void fft_pass(cplx (&x)[16], uint32_t tau, c
         } else {
             const uint32_t base = (j >> NS_LOG) * (NS * R) + k;
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const uint32_t pos = spad(base + r * NS);
-                sre[pos] = v[r].x;
-                sim[pos] = v[r].y;
-            }
+            for (int r = 0; r < R; ++r) ex.store(spad(base + r * NS), v[r]);
         }
     }
 }
 
-// Gather this thread's 16 elements (tau + m*N/16) back from shared memory.
-template <int LOGN>
-__host__ __device__ __forceinline__ void fft_gather(cplx (&x)[16], uint32_t tau, const float* sre, const float* sim)
+template <int LOGN, int P, int SIGN>
+__host__ __device__ __forceinline__ void fft_pass(cplx (&x)[16], uint32_t tau, const cplx* __restrict__ tw,
+                                                  float* sre, float* sim, const BaseTwiddles<LOGN>& wb)
+{
+    fft_pass_ex<LOGN, P, SIGN>(x, tau, tw, ShmemPair{sre, sim}, wb);
+}
+
+// Gather this thread's 16 elements (tau + m*N/16) back from the exchange arrays.
+template <int LOGN, class EX>
+__host__ __device__ __forceinline__ void fft_gather_ex(cplx (&x)[16], uint32_t tau, const EX& ex)
 {
     constexpr int TPF = (1 << LOGN) / 16;
 #pragma unroll
-    for (int m = 0; m < 16; ++m) {
-        const uint32_t pos = spad(tau + m * TPF);
-        x[m] = {sre[pos], sim[pos]};
-    }
+    for (int m = 0; m < 16; ++m) x[m] = ex.load(spad(tau + m * TPF));
+}
+
+template <int LOGN>
+__host__ __device__ __forceinline__ void fft_gather(cplx (&x)[16], uint32_t tau, const float* sre, const float* sim)
+{
+    fft_gather_ex<LOGN>(x, tau, ShmemPair{const_cast<float*>(sre), const_cast<float*>(sim)});
 }
 
 // ---- Two transforms at once on paired FP32 lanes ----------------------------------------------

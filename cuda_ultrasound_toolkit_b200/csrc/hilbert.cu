@@ -27,6 +27,7 @@
 #include <complex>
 #include <vector>
 
+#include <cooperative_groups.h>
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -197,6 +198,123 @@ bool launch_hilbert_t(const float* in, void* out, const HilbertArgs& a, cudaStre
     return true;
 }
 
+// ---- Rows longer than one CTA holds: a thread-block cluster per row --------------------------
+// A CTA's shared memory holds the exchange arrays of 2^14 points (2 x 64 KiB). A row of N = 2^15 ..
+// 2^17 points is transformed by a cluster of R = N / 2^14 CTAs of 1024 threads: CTA r runs threads
+// tau = 1024 r .. 1024 r + 1023 of the N/16-thread Stockham transform (the same passes as the
+// one-CTA kernels) and holds positions r 2^14 .. (r + 1) 2^14 - 1 of the exchange arrays; the passes
+// store to and gather from the owning CTA through distributed shared memory, and cluster barriers
+// separate the phases. One real row per cluster: iq = IDFT(X G) with G = Ge + i Go.
+namespace cg = cooperative_groups;
+constexpr int kSliceLog = 14;                        // exchange positions per CTA: 2^14
+constexpr uint32_t kSlice = 1u << kSliceLog;
+constexpr int kClusterThreads = (int)(kSlice / 16);  // 1024
+
+// The exchange arrays spread over the cluster: position pos lives in CTA pos >> 14 at offset
+// pos & (2^14 - 1) of its `re` / `im` arrays (the swizzle of fft::spad keeps a position in its slice).
+struct ClusterExchange {
+    float* re;  // this CTA's arrays (the same offsets in every CTA of the cluster)
+    float* im;
+    __device__ __forceinline__ void store(uint32_t pos, cplx v) const
+    {
+        cg::cluster_group cl = cg::this_cluster();
+        const unsigned rank = pos >> kSliceLog, off = pos & (kSlice - 1);
+        *cl.map_shared_rank(re + off, rank) = v.x;
+        *cl.map_shared_rank(im + off, rank) = v.y;
+    }
+    __device__ __forceinline__ cplx load(uint32_t pos) const
+    {
+        cg::cluster_group cl = cg::this_cluster();
+        const unsigned rank = pos >> kSliceLog, off = pos & (kSlice - 1);
+        return {*cl.map_shared_rank(re + off, rank), *cl.map_shared_rank(im + off, rank)};
+    }
+};
+
+template <int LOGN, int SIGN, int P = 0>
+__device__ __forceinline__ void run_fft_cluster(cplx (&x)[16], uint32_t tau, const cplx* tw, const ClusterExchange& ex,
+                                                const fft::BaseTwiddles<LOGN>& wb)
+{
+    constexpr int NP = fft::pass_count(LOGN);
+    if constexpr (P < NP) {
+        fft::fft_pass_ex<LOGN, P, SIGN>(x, tau, tw, ex, wb);
+        if constexpr (P < NP - 1) {
+            cg::this_cluster().sync();  // every store of the pass is visible cluster-wide
+            fft::fft_gather_ex<LOGN>(x, tau, ex);
+            cg::this_cluster().sync();  // every gather is done before the next pass stores
+        }
+        run_fft_cluster<LOGN, SIGN, P + 1>(x, tau, tw, ex, wb);
+    }
+}
+
+template <int LOGN, class OutT, bool PAD>
+__global__ void __launch_bounds__(kClusterThreads, 1)
+hilbert_cluster_kernel(const float* __restrict__ in, OutT* __restrict__ out, HilbertArgs a)
+{
+    constexpr uint32_t N = 1u << LOGN;
+    constexpr uint32_t TPF = N / 16;
+    constexpr uint32_t R = N >> kSliceLog;
+    static_assert(R >= 2 && R <= 8, "clusters of 2 .. 8 CTAs");
+    extern __shared__ float smem[];
+    cg::cluster_group cl = cg::this_cluster();
+    const uint32_t rank = cl.block_rank();
+    const uint32_t tau = rank * kClusterThreads + threadIdx.x;
+    const uint64_t row = blockIdx.x / R;
+    const uint32_t L = PAD ? a.n : N;
+    const bool has_row = row < a.rows;
+    const ClusterExchange ex{smem, smem + kSlice};
+    const cplx* tw = reinterpret_cast<const cplx*>(a.twiddle);
+    fft::BaseTwiddles<LOGN> wb;
+    fft::load_base_twiddles<LOGN>(wb, tau, tw);
+    cplx z[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const uint64_t n = tau + m * TPF;
+        z[m].x = has_row && (!PAD || n < L) ? __ldcs(in + (row * L + n) * a.in_stride) : 0.f;
+        z[m].y = 0.f;
+    }
+    cl.sync();  // every CTA of the cluster runs before any shared memory of another is written
+    run_fft_cluster<LOGN, -1>(z, tau, tw, ex, wb);
+    const float4* wt = reinterpret_cast<const float4*>(a.weight);
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const float4 w = __ldg(wt + tau + m * TPF);
+        z[m] = fft::cmul(z[m], cplx{w.x - w.w, w.z + w.y});
+    }
+    run_fft_cluster<LOGN, +1>(z, tau, tw, ex, wb);
+    // The last shared-memory accesses ended at a cluster barrier, so no CTA leaves while another
+    // still reads its arrays.
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const uint64_t n = tau + m * TPF;
+        if (has_row && (!PAD || n < L)) store_iq(out, row * L + n, z[m].x, z[m].y);
+    }
+}
+
+template <int LOGN, class OutT, bool PAD>
+bool launch_hilbert_cluster(const float* in, void* out, const HilbertArgs& a, cudaStream_t st)
+{
+    constexpr unsigned R = 1u << (LOGN - kSliceLog);
+    constexpr size_t smem = 2 * kSlice * sizeof(float);
+    auto kern = hilbert_cluster_kernel<LOGN, OutT, PAD>;
+    static std::atomic<uint64_t> smem_set{0};
+    if (!set_smem_limit(kern, smem, smem_set)) return false;
+    CUTB_REQUIRE(a.rows * R <= 0x7fffffffull, CUTB_ERR_INVALID_ARGUMENT, "Too many rows for one launch.");
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(a.rows * R));
+    cfg.blockDim = dim3(kClusterThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = R;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CUTB_CUDA_OK(cudaLaunchKernelEx(&cfg, kern, in, (OutT*)out, a));
+    return true;
+}
+
 template <class OutT, bool PAD>
 bool launch_hilbert_o(const float* in, void* out, const HilbertArgs& a, cudaStream_t st)
 {
@@ -212,6 +330,9 @@ bool launch_hilbert_o(const float* in, void* out, const HilbertArgs& a, cudaStre
         case 12: return launch_hilbert_t<12, OutT, PAD>(in, out, a, st);
         case 13: return launch_hilbert_t<13, OutT, PAD>(in, out, a, st);
         case 14: return launch_hilbert_t<14, OutT, PAD>(in, out, a, st);
+        case 15: return launch_hilbert_cluster<15, OutT, PAD>(in, out, a, st);
+        case 16: return launch_hilbert_cluster<16, OutT, PAD>(in, out, a, st);
+        case 17: return launch_hilbert_cluster<17, OutT, PAD>(in, out, a, st);
         default: break;
     }
     set_error(CUTB_ERR_UNSUPPORTED, "Hilbert transform length 2^%u not supported.", a.log_n);

@@ -27,7 +27,6 @@ namespace cutb {
 namespace {
 
 constexpr unsigned kStaticMaxSamples = 16384;
-static_assert(kStaticMaxSamples >= kMaxHilbertLength, "the array must hold the longest transform's tables");
 constexpr int kMaxDevices = 64;
 
 // twiddle (kStaticMaxSamples complex values) | spectral weight (kStaticMaxSamples x 4 floats).
@@ -71,6 +70,9 @@ extern "C" CUTB_API bool cutb_hilbert_static(const float* d_in, uint in_stride, 
     CUTB_REQUIRE(hilbert_supported_length(samples), CUTB_ERR_UNSUPPORTED,
                  "Sample count %u not supported by the FFT (powers of two up to %u, other lengths up to %u).",
                  samples, kMaxHilbertLength, kMaxHilbertLength / 2);
+    CUTB_REQUIRE(hilbert_fft_length(samples) <= kStaticMaxSamples, CUTB_ERR_INVALID_ARGUMENT,
+                 "cutb_hilbert_static: %u samples per row need a transform of %u points, above the fixed table "
+                 "capacity of %u.", samples, hilbert_fft_length(samples), kStaticMaxSamples);
     CUTB_REQUIRE(ntaps == 0 || taps, CUTB_ERR_INVALID_ARGUMENT, "Null match filter.");
     // The table upload copies from host vectors that are freed when the call returns, so a graph
     // captured from it would replay reads of freed memory: capture is refused.

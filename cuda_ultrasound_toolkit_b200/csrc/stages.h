@@ -54,7 +54,7 @@ struct DemodArgs {
 bool launch_demod_fir(const DemodArgs& a, const float* in, void* out, bool bf16, cudaStream_t st);
 
 // ---- analytic signal (hilbert.cu) --------------------------------------------------------
-constexpr unsigned kMaxHilbertLength = 16384;
+constexpr unsigned kMaxHilbertLength = 131072;
 
 struct HilbertArgs {
     uint64_t rows;             // T * C rows of n samples

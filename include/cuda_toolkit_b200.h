@@ -97,8 +97,9 @@ CUTB_API bool cutb_decode(cutb_plan* plan, const void* d_raw, size_t raw_bytes, 
 
 /* Match-filtered analytic signal of every [T][C] row: d_in f32 with element stride in_stride
  * (1 = packed, 2 = real part of complex) -> d_iq complex [T][C][S] (complex64, or bf16x2
- * when the plan stores bf16). S: any power of two up to 16384, any other count up to 8192
- * (computed as a zero-padded circular convolution of the same result); longer rows report
+ * when the plan stores bf16). S: any power of two up to 131072, any other count up to 65536
+ * (computed as a zero-padded circular convolution of the same result); rows of more than 16384
+ * transform points run on a thread-block cluster of 2 to 8 CTAs per row. Longer rows report
  * CUTB_ERR_UNSUPPORTED. */
 CUTB_API bool cutb_hilbert(cutb_plan* plan, const float* d_in, uint in_stride, void* d_iq, void* stream);
 
@@ -180,8 +181,8 @@ CUTB_API int cutb_plan_last_launch_count(const cutb_plan* plan);
  * match filter in host memory (ntaps <= samples, 0 = none). The FFT tables live in a fixed device
  * array sized for transforms of up to 16384 points (384 KiB, held by every GPU that loads the
  * library until the process exits): rows of up to 16384 samples when the count is a power of two,
- * up to 8192 otherwise. Rows longer than 16384 are rejected with CUTB_ERR_INVALID_ARGUMENT, other
- * unsupported counts with CUTB_ERR_UNSUPPORTED. A call on a stream that is being captured into a
+ * up to 8192 otherwise. Rows beyond that capacity are rejected with CUTB_ERR_INVALID_ARGUMENT,
+ * counts no transform supports with CUTB_ERR_UNSUPPORTED. A call on a stream that is being captured into a
  * CUDA graph is rejected with CUTB_ERR_UNSUPPORTED: the tables are uploaded from host memory that
  * the call frees before a graph could replay the copy. Every call rewrites the array on `stream`;
  * calls that overlap on the GPU race on it and must be serialised. */

@@ -125,6 +125,28 @@ def test_hilbert_vs_fp64(torch, orc, N, taps):
     assert rel_l2(got, ref) < TOL_HILBERT
 
 
+# Rows of more than 2^14 transform points: a thread-block cluster of 2, 4 or 8 CTAs per row (the
+# exchange arrays spread over their shared memory). 8193 samples pad to 32768 (the oracle's DFT of a
+# length that is not a power of two is a direct sum, so that case keeps to one row).
+@pytest.mark.parametrize("N,rows,taps", [(32768, 2, 0), (32768, 2, 64), (65536, 2, 64), (131072, 2, 64),
+                                         (131072, 1, 0), (8193, 1, 64)])
+def test_hilbert_cluster_lengths_vs_fp64(torch, orc, N, rows, taps):
+    rng = np.random.default_rng(N + taps + rows)
+    x = rng.normal(size=(1, rows, N)).astype(np.float32)
+    bp = base_params(N, rows, 1, decode=EncodingMatrix.NONE)
+    h = None
+    if taps:
+        h = synth.chirp_taps(taps)
+        bp.filter_length = len(h)
+        for i, v in enumerate(h):
+            bp.rf_filter[i] = float(v)
+    plan = Plan(bp)
+    got = plan.hilbert(torch.from_numpy(x).cuda()).cpu().numpy()
+    plan.check()
+    ref = orc.hilbert(x.astype(np.float64), h)
+    assert rel_l2(got, ref) < TOL_HILBERT
+
+
 def test_hilbert_strided_input_and_known_answer(torch, orc):
     N, T, C = 1024, 2, 2
     n = np.arange(N)
@@ -474,10 +496,10 @@ def test_invalid_parameters_are_rejected(torch):
         with pytest.raises(CutbError) as e:
             Plan(bp)
         assert e.value.code == code, e.value
-    # decode works, the FFT length does not (not a power of two, and over 8192)
-    plan = Plan(base_params(8196, C, T))
+    # decode works, the FFT length does not (not a power of two, and over 65536)
+    plan = Plan(base_params(65537, C, T))
     with pytest.raises(CutbError) as e:
-        plan.beamform(torch.zeros(8196 * T * C, dtype=torch.int16, device="cuda"))
+        plan.beamform(torch.zeros(65537 * T * C, dtype=torch.int16, device="cuda"))
     assert e.value.code == 2
 
 

@@ -84,6 +84,9 @@ def test_static_hilbert_rejects_rows_beyond_capacity():
     buf = torch.zeros(16, dtype=torch.float32, device="cuda")
     assert not fn(buf.data_ptr(), 1, buf.data_ptr(), 32768, 1, None, 0, None)
     assert lib().cutb_last_error() == 1
+    # 10000 samples would need a transform of 32768 points: also beyond the fixed tables
+    assert not fn(buf.data_ptr(), 1, buf.data_ptr(), 10000, 1, None, 0, None)
+    assert lib().cutb_last_error() == 1
 
 
 def test_static_hilbert_refuses_stream_capture():
