@@ -65,6 +65,24 @@ def test_motion_parameter_layout(tmp_path):
     assert vals[-2:] == [ctypes.sizeof(NccMotionParameters), ctypes.sizeof(CorrImagesParameters)]
 
 
+def test_plan_options_layout(tmp_path):
+    """cutb_options: the ctypes mirror the Python layer passes to cutb_plan_create matches the C
+    header (every named field's offset and the struct size)."""
+    from cuda_ultrasound_toolkit_b200.api import _Options
+    fields = [f[0] for f in _Options._fields_ if f[0] != "reserved"]
+    src = tmp_path / "o.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "cuda_toolkit_b200.h"\n'
+                   "int main(void) {\n"
+                   + "".join(f'printf("%zu\\n", offsetof(cutb_options, {f}));\n' for f in fields)
+                   + 'printf("%zu\\n", sizeof(cutb_options));\n'
+                   "return 0; }\n")
+    exe = tmp_path / "o"
+    subprocess.run(["gcc", "-std=c11", "-I", INCLUDE, str(src), "-o", str(exe)], check=True)
+    vals = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
+    assert vals[:-1] == [getattr(_Options, f).offset for f in fields]
+    assert vals[-1] == ctypes.sizeof(_Options) == 64
+
+
 def _declared_functions(only=None, skip=("cuda_transfer.h",)):
     names = set()
     for fn in os.listdir(INCLUDE):
