@@ -212,37 +212,54 @@ constexpr int kClusterThreads = (int)(kSlice / 16);  // 1024
 
 // The exchange arrays spread over the cluster: position pos lives in CTA pos >> 14 at offset
 // pos & (2^14 - 1) of its `re` / `im` arrays (the swizzle of fft::spad keeps a position in its slice).
+// Addresses stay 32-bit: this CTA's shared-memory address of the offset is mapped to the owning
+// CTA's in the cluster window (mapa), and the access goes to that window directly.
+__device__ __forceinline__ uint32_t cluster_address(uint32_t local, uint32_t rank)
+{
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
+    return r;
+}
 struct ClusterExchange {
-    float* re;  // this CTA's arrays (the same offsets in every CTA of the cluster)
-    float* im;
+    uint32_t re;  // shared-memory addresses of this CTA's arrays (the same offsets in every CTA)
+    uint32_t im;
     __device__ __forceinline__ void store(uint32_t pos, cplx v) const
     {
-        cg::cluster_group cl = cg::this_cluster();
-        const unsigned rank = pos >> kSliceLog, off = pos & (kSlice - 1);
-        *cl.map_shared_rank(re + off, rank) = v.x;
-        *cl.map_shared_rank(im + off, rank) = v.y;
+        const uint32_t rank = pos >> kSliceLog, off = (pos & (kSlice - 1)) * 4u;
+        asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(cluster_address(re + off, rank)), "f"(v.x) : "memory");
+        asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(cluster_address(im + off, rank)), "f"(v.y) : "memory");
     }
     __device__ __forceinline__ cplx load(uint32_t pos) const
     {
-        cg::cluster_group cl = cg::this_cluster();
-        const unsigned rank = pos >> kSliceLog, off = pos & (kSlice - 1);
-        return {*cl.map_shared_rank(re + off, rank), *cl.map_shared_rank(im + off, rank)};
+        const uint32_t rank = pos >> kSliceLog, off = (pos & (kSlice - 1)) * 4u;
+        cplx v;
+        asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v.x) : "r"(cluster_address(re + off, rank)) : "memory");
+        asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v.y) : "r"(cluster_address(im + off, rank)) : "memory");
+        return v;
     }
 };
 
+// The cluster kernel runs at 64 registers a thread: each pass loads its two base twiddles (w^k and
+// w^(4k), read through the cache) just before it instead of holding every pass's for the kernel.
 template <int LOGN, int SIGN, int P = 0>
-__device__ __forceinline__ void run_fft_cluster(cplx (&x)[16], uint32_t tau, const cplx* tw, const ClusterExchange& ex,
-                                                const fft::BaseTwiddles<LOGN>& wb)
+__device__ __forceinline__ void run_fft_cluster(cplx (&x)[16], uint32_t tau, const cplx* tw, const ClusterExchange& ex)
 {
     constexpr int NP = fft::pass_count(LOGN);
     if constexpr (P < NP) {
+        fft::BaseTwiddles<LOGN> wb;
+        if constexpr (P > 0 && fft::pass_radix(LOGN, P) == 16) {
+            constexpr int sh = LOGN - fft::pass_ns_log(LOGN, P) - 4;
+            const uint32_t k = tau & ((1u << fft::pass_ns_log(LOGN, P)) - 1);
+            wb.w[P][0] = tw[k << sh];
+            wb.w[P][1] = tw[(4 * k) << sh];
+        }
         fft::fft_pass_ex<LOGN, P, SIGN>(x, tau, tw, ex, wb);
         if constexpr (P < NP - 1) {
             cg::this_cluster().sync();  // every store of the pass is visible cluster-wide
             fft::fft_gather_ex<LOGN>(x, tau, ex);
             cg::this_cluster().sync();  // every gather is done before the next pass stores
         }
-        run_fft_cluster<LOGN, SIGN, P + 1>(x, tau, tw, ex, wb);
+        run_fft_cluster<LOGN, SIGN, P + 1>(x, tau, tw, ex);
     }
 }
 
@@ -261,10 +278,9 @@ hilbert_cluster_kernel(const float* __restrict__ in, OutT* __restrict__ out, Hil
     const uint64_t row = blockIdx.x / R;
     const uint32_t L = PAD ? a.n : N;
     const bool has_row = row < a.rows;
-    const ClusterExchange ex{smem, smem + kSlice};
+    const uint32_t base = (uint32_t)__cvta_generic_to_shared(smem);
+    const ClusterExchange ex{base, base + kSlice * 4u};
     const cplx* tw = reinterpret_cast<const cplx*>(a.twiddle);
-    fft::BaseTwiddles<LOGN> wb;
-    fft::load_base_twiddles<LOGN>(wb, tau, tw);
     cplx z[16];
 #pragma unroll
     for (int m = 0; m < 16; ++m) {
@@ -273,14 +289,14 @@ hilbert_cluster_kernel(const float* __restrict__ in, OutT* __restrict__ out, Hil
         z[m].y = 0.f;
     }
     cl.sync();  // every CTA of the cluster runs before any shared memory of another is written
-    run_fft_cluster<LOGN, -1>(z, tau, tw, ex, wb);
+    run_fft_cluster<LOGN, -1>(z, tau, tw, ex);
     const float4* wt = reinterpret_cast<const float4*>(a.weight);
 #pragma unroll
     for (int m = 0; m < 16; ++m) {
         const float4 w = __ldg(wt + tau + m * TPF);
         z[m] = fft::cmul(z[m], cplx{w.x - w.w, w.z + w.y});
     }
-    run_fft_cluster<LOGN, +1>(z, tau, tw, ex, wb);
+    run_fft_cluster<LOGN, +1>(z, tau, tw, ex);
     // The last shared-memory accesses ended at a cluster barrier, so no CTA leaves while another
     // still reads its arrays.
 #pragma unroll
