@@ -158,11 +158,12 @@ def voxel_subset(bp, k, n=N_VOXEL_SUBSETS, seed=0):
     return np.sort(np.array_split(perm, n)[k % n])
 
 
-def cpu_sample(raw, bp, threads, subset=0, n_subsets=N_VOXEL_SUBSETS, channels=None, keep_iq=False):
+def cpu_sample(raw, bp, threads, subset=0, n_subsets=N_VOXEL_SUBSETS, channels=None, keep_iq=False, elapsed=None):
     """Times the FP64 oracle on one bounded sample of a frame and extrapolates seconds per volume:
     convert + decode and the Hilbert analytic signal of `channels` receive channels (default: all,
     i.e. the front end in full), and the delay-and-sum of voxel subset `subset` of `n_subsets`
-    (scaled by n_subsets). Returns (seconds per volume, description, analytic signal or None)."""
+    (scaled by n_subsets). Returns (seconds per volume, description, analytic signal or None); the
+    sample's own duration is appended to the list `elapsed` when one is given."""
     from oracle import oracle as O
     S, C, T = bp.dims
     z, y, x = bp.volume_shape
@@ -183,6 +184,8 @@ def cpu_sample(raw, bp, threads, subset=0, n_subsets=N_VOXEL_SUBSETS, channels=N
     O.das(iq, bp, vox, threads)
     t4 = time.perf_counter()
     per_volume = (t2 - t0) * C / sub_c + (t4 - t3) * (x * y * z) / len(vox)
+    if elapsed is not None:
+        elapsed.append((t2 - t0) + (t4 - t3))
     front = "in full" if sub_c == C else f"on {sub_c} of {C} receive channels, scaled"
     sample = (f"FP64 oracle: convert + decode + Hilbert of {T} x {C} rows x {S} samples {front}; "
               f"delay-and-sum of the seeded voxel subset {subset % n_subsets} of {n_subsets} ({len(vox)} of "
@@ -198,14 +201,18 @@ def run_reference(args, rank):
     threads = os.cpu_count() or 1
     for k in range(args.warmup):  # untimed: a light pass over the same code
         cpu_sample(raw, bp, threads, subset=k, n_subsets=4096, channels=8)
-    times = []
+    # A step is one bounded sample (the front end in full, 1/64 of the voxels): ms_per_step is its
+    # measured duration, and value extrapolates the samples to whole volumes per second.
+    times, ran = [], []
     sample = ""
     for k in range(args.steps):
-        sec, sample, _ = cpu_sample(raw, bp, threads, subset=k)
+        sec, sample, _ = cpu_sample(raw, bp, threads, subset=k, elapsed=ran)
         times.append(sec)
     value = len(times) / sum(times)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(ran) / len(ran),
+            "step": "one bounded sample of the frame (front end in full, delay-and-sum of 1/64 of the voxels); "
+                    f"{1e3 * sum(times) / len(times):.0f} ms per volume extrapolated",
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded phantom, 200 point scatterers, 40 dB SNR)",
             "config": workload_config({"parallelism": parallelism(int(os.environ.get("WORLD_SIZE", "1")))}),
