@@ -791,7 +791,6 @@ def sequences_section(reps=5, warmup=3, seed=11):
     pairs, then demodulation + filter, both HBM-bound."""
     import torch
     from cuda_ultrasound_toolkit_b200 import Plan, synth
-    from cuda_ultrasound_toolkit_b200.params import SequenceId
     from oracle import oracle as O
     threads = os.cpu_count() or 1
     rng = np.random.default_rng(seed)
@@ -801,23 +800,9 @@ def sequences_section(reps=5, warmup=3, seed=11):
     # 32-voxel-wide tile overflow, so the default engine is one thread per voxel); "_fine": a 9.6 mm
     # wide volume (x step 0.038 mm), on the staged engine
     for name in ("tpw", "uforces", "tpw_fine", "uforces_fine"):
-        half = (C * synth.PITCH / 2) if not name.endswith("_fine") else 4.8e-3
-        w = synth.Workload(name, T, C, S, X, 1, Z, 0, cubic=True, cf=1.0)
-        bp = synth.make_params(w)
-        bp.tx_orientation = bp.rx_orientation  # x-z plane
-        bp.output_min_coordinate[0], bp.output_max_coordinate[0] = -half, half
-        bp.fn_rx = 1.0
-        if name.startswith("tpw"):
-            bp.das_shader_id = int(SequenceId.RCA_TPW)
-            for t, ang in enumerate(np.linspace(-0.25, 0.25, T)):
-                bp.foci[3 * t + 2] = float(ang)
-            used = T
-        else:
-            bp.das_shader_id = int(SequenceId.UFORCES)
-            bp.foci[2] = 30e-3
-            for t in range(T):
-                bp.sparse_elements[t] = 2 * t
-            used = T - 1  # transmit row 0 (the flash) is not summed
+        bp = synth.sequence_params(name, T, C, S, X, Z)
+        half = -bp.output_min_coordinate[0]
+        used = T if name.startswith("tpw") else T - 1  # UFORCES: transmit row 0 (the flash) is not summed
         plan = Plan(bp)
         iq = torch.complex(torch.randn(T, C, S, device="cuda"), torch.randn(T, C, S, device="cuda"))
         vol = plan.empty_volume()

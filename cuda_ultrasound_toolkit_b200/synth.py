@@ -58,6 +58,32 @@ CONFIGS = {
 }
 
 
+def sequence_params(name, T=64, C=128, S=2048, X=256, Z=512):
+    """The tilted-plane-wave and UFORCES workloads of the benchmark's sequence section: T transmits x
+    C channels x S samples -> X x 1 x Z (x, y, z), cubic + coherence factor, receive Hann window of
+    f-number 1, in the x-z plane (y-invariant). "tpw": plane waves at angles linspace(-0.25, 0.25)
+    rad; "uforces": transmit t on element 2t, focus at 30 mm (transmit 0 is the flash). The plain
+    names span the whole aperture in x (0.15 mm steps: the staged windows of a 32-voxel-wide tile
+    overflow); "_fine" spans x in +-4.8 mm (0.038 mm steps), on the staged engine."""
+    half = (C * PITCH / 2) if not name.endswith("_fine") else 4.8e-3
+    bp = make_params(Workload(name, T, C, S, X, 1, Z, 0, cubic=True, cf=1.0))
+    bp.tx_orientation = bp.rx_orientation  # x-z plane
+    bp.output_min_coordinate[0], bp.output_max_coordinate[0] = -half, half
+    bp.fn_rx = 1.0
+    if name.startswith("tpw"):
+        bp.das_shader_id = int(SequenceId.RCA_TPW)
+        for t, ang in enumerate(np.linspace(-0.25, 0.25, T)):
+            bp.foci[3 * t + 2] = float(ang)
+    elif name.startswith("uforces"):
+        bp.das_shader_id = int(SequenceId.UFORCES)
+        bp.foci[2] = 30e-3
+        for t in range(T):
+            bp.sparse_elements[t] = 2 * t
+    else:
+        raise ValueError(f"unknown sequence workload {name!r}")
+    return bp
+
+
 def chirp_taps(n, f0=3e6, f1=7e6, fs=FS):
     """Linear chirp f0 -> f1 over n samples with a Hann taper, unit energy."""
     t = np.arange(n) / fs
